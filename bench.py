@@ -1,0 +1,447 @@
+#!/usr/bin/env python3
+"""Benchmark of the streamline-tracking hot path on B200.
+
+Workload (single GPU): the plain Diffusion configuration -- a synthetic
+145 x 174 x 145 spherical-harmonic FOD (lmax 8, 45 float32 coefficients,
+1.25 mm voxels, about 660 MB), seeds drawn by ``seeds.from_fod`` with a
+fixed NumPy seed, Diffusion with step 0.001 mm, gamma 1, noise variance 0.1,
+save_at 0.25 mm, maximum length 300 mm, batches of 50 000 seeds.  One
+benchmark step is one batch: the reference's unit of work, one
+``tracking.tractogram`` call.
+
+Metric: streamline-steps/s, where a step is one iteration of the tracking
+loop that passed both the domain and the field check (tracking.py:121-147).
+
+Reported:
+  value     device-resident throughput: seeds already in HBM, one
+            persistent-tracker run per batch, packed output left on the
+            device; CUDA events on the tracker's stream, max over ranks.
+  e2e       the same metric through the C ABI with host buffers: the
+            host-to-device copy of the batch's seeds, tracking, and the
+            device-to-host copy of lengths, offsets and packed points are
+            all inside the timed region.
+  roofline  the tracking kernel's algorithmic bytes per step
+            (4 C + 4 + 16 step/save_at = 184.064 B at C = 45) times the
+            steps of a launch over its event-timed duration, against the
+            measured HBM copy bandwidth.
+  cpu_baseline  the CPU oracle (plain-C restatement of the reference
+            kernel, OpenMP over seeds) on a bounded sample of the same
+            workload on this host's cores.
+
+``--impl reference`` times the reference's CPU path instead (the compiled
+reference kernels under oracle/_ref when present, else the oracle) and
+prints the same JSON line with "impl": "reference".
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "streamline-steps/s"
+UNIT = "steps/s"
+C = 45
+STEP = 0.001
+SAVE_AT = 0.25
+MAX_LENGTH = 300.0
+GAMMA = 1.0
+NOISE = 0.1
+BYTES_PER_STEP = 4 * C + 4 + 16 * STEP / SAVE_AT
+WORKLOAD = ("config1 Diffusion: SH lmax 8 (45 f32 coefficients) 145x174x145 at 1.25 mm, 3 bundles; "
+            "seeds from seeds.from_fod; step 0.001 mm, gamma 1, noise_variance 0.1; save_at 0.25, "
+            "max length 300 mm; batch 50000 seeds per step")
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--batch", type=int, default=50000)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_step():
+    """DRAM bytes per accepted step of the tracking kernel from the committed ncu summary."""
+    path = ROOT / "profiles" / "track_persistent_config1.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith("dram_bytes_per_step:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        rows = []
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[4:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = np.array([r[0] for r in rows])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for _, _, flags in rows:
+            for name, flag in zip(names, flags[1:]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][1]), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def setup_workload(rank: int, n_seeds: int, runtime):
+    import tractography_b200 as tg
+    from tractography_b200 import synthetic
+
+    fod = synthetic.config1(seed=0)
+    field = tg.field.Image(fod)
+    mask = np.any(field.values != 0, axis=-1).astype(np.uint8)
+    domain = tg.domain.Image(tg.Nifti1Image(mask, fod.affine))
+    state = np.random.get_state()
+    np.random.seed(2024 + rank)
+    try:
+        seeds = tg.seeds.from_fod(fod, n_seeds, runtime=runtime)
+    finally:
+        np.random.set_state(state)
+    model = tg.local.RealSymmetricSphericalHarmonics(C)
+    algorithm = tg.algorithm.Diffusion(model, step_size=STEP, gamma=GAMMA, noise_variance=NOISE, seed=1234 + rank)
+    return fod, field, domain, seeds, algorithm
+
+
+def run_ours(args):
+    import torch
+
+    import tractography_b200 as tg
+    from tractography_b200 import _lib
+    from tractography_b200.algorithm import to_struct
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local_rank)
+    runtime = tg.CudaRuntime(local_rank)
+    lib = runtime.lib
+    n_total = args.batch * (args.warmup + args.steps)
+    fod, field, domain, seeds, algorithm = setup_workload(rank, n_total, runtime)
+    n_steps = int(math.floor(MAX_LENGTH / SAVE_AT))
+    batches = [np.ascontiguousarray(seeds[i * args.batch:(i + 1) * args.batch]) for i in range(args.warmup + args.steps)]
+    rng_seeds = [np.array([algorithm.get_rng_seed()], dtype=np.uint32) for _ in batches]
+    stream = runtime.stream
+    sh = ctypes.c_void_p(runtime.stream_handle)
+    with runtime.device_scope():
+        d_handle = domain.device(runtime)
+        f_handle = field.device(runtime, _lib.MODEL_SH)
+        tracker = runtime.tracker()
+        a = to_struct(algorithm)
+        dev_batches = [runtime.to_device(b) for b in batches]
+        host_batches = []
+        for b in batches:
+            pb = runtime.pinned(b.shape, np.float32)
+            pb[...] = b
+            host_batches.append(pb)
+        torch.cuda.synchronize()
+        lengths = np.empty(args.batch, np.uint32)
+        offsets = np.empty(args.batch, np.uint64)
+        total = ctypes.c_uint64()
+        steps = ctypes.c_uint64()
+        kms = ctypes.c_float()
+        waves = ctypes.c_uint32()
+        launches = ctypes.c_uint32()
+
+        def run(i, on_host):
+            src = host_batches[i] if on_host else dev_batches[i]
+            ptr = src.ctypes.data_as(ctypes.c_void_p) if on_host else ctypes.c_void_p(src.data_ptr())
+            _lib.check(lib.tg_tracker_run(
+                tracker, ctypes.byref(a), d_handle, f_handle, ptr, 1 if on_host else 0, args.batch, args.batch,
+                rng_seeds[i].ctypes.data_as(ctypes.c_void_p), SAVE_AT, n_steps,
+                lengths.ctypes.data_as(ctypes.c_void_p), offsets.ctypes.data_as(ctypes.c_void_p),
+                ctypes.byref(total), ctypes.byref(steps), sh))
+            _lib.check(lib.tg_tracker_stats(tracker, ctypes.byref(kms), ctypes.byref(waves), ctypes.byref(launches)))
+            return int(steps.value), int(total.value), float(kms.value), int(launches.value), int(waves.value)
+
+        out_host = runtime.pinned((args.batch * n_steps, 3), np.float32)
+
+        for i in range(args.warmup):
+            run(i, on_host=False)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        sampler = ClockSampler(local_rank)
+        with sampler:
+            # device-resident leg
+            if dist is not None:
+                dist.barrier()
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            dev_steps = dev_points = n_launch = n_waves = 0
+            kernel_ms = 0.0
+            for i in range(args.warmup, args.warmup + args.steps):
+                s, p, k, nl, nw = run(i, on_host=False)
+                dev_steps += s
+                dev_points += p
+                kernel_ms += k
+                n_launch += nl
+                n_waves += nw
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            dev_ms = ev0.elapsed_time(ev1)
+            if dist is not None:
+                dist.barrier()
+
+            # end-to-end leg through the C ABI with host buffers
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            e2e_steps = 0
+            h2d = d2h = 0
+            for i in range(args.warmup, args.warmup + args.steps):
+                s, p, _, _, _ = run(i, on_host=True)
+                _lib.check(lib.tg_tracker_copy_points(tracker, out_host.ctypes.data_as(ctypes.c_void_p), 0, p, 1, sh))
+                e2e_steps += s
+                h2d += batches[i].nbytes + 4
+                d2h += p * 12 + args.batch * (4 + 8)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms = ev0.elapsed_time(ev1)
+            if dist is not None:
+                dist.barrier()
+
+    if dist is not None:
+        t = torch.tensor([dev_ms, e2e_ms, kernel_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        c = torch.tensor([dev_steps, e2e_steps, dev_points, n_launch, n_waves], dtype=torch.float64, device="cuda")
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        dev_ms, e2e_ms, kernel_ms = (float(x) for x in t.tolist())
+        dev_steps, e2e_steps, dev_points, n_launch, n_waves = (int(x) for x in c.tolist())
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = measured_peaks()
+    value = dev_steps / (dev_ms / 1e3)
+    kernel_steps_per_s = dev_steps / max(1, world) / (kernel_ms / 1e3)
+    achieved = kernel_steps_per_s * BYTES_PER_STEP / 1e9
+    tps = traffic_per_step()
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generator; no dataset)",
+        "config": {
+            "workload": WORKLOAD,
+            "batch_seeds": args.batch,
+            "max_points_per_streamline": n_steps,
+            "cache": "inputs larger than L2: 660 MB FOD volume, 126 MB L2",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "rng": "MWC64X reference stream per batch",
+        },
+        "streamlines_per_s": args.batch * args.steps * world / (dev_ms / 1e3),
+        "points_per_step": dev_points / args.steps / max(1, world),
+        "e2e": {
+            "value": e2e_steps / (e2e_ms / 1e3),
+            "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d / args.steps),
+            "d2h_bytes_per_step": int(d2h / args.steps),
+        },
+        "gpu_launches": n_launch,
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": (tps * dev_steps / max(1, n_waves)) if tps is not None else None,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "bytes_per_step": BYTES_PER_STEP,
+            "kernel_ms_per_step": kernel_ms / args.steps / max(1, world),
+        },
+        "clocks": sampler.summary(),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(field, domain, seeds[args.warmup * args.batch:])
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def _reference_lib():
+    """The compiled reference kernels (oracle/_ref), or None."""
+    path = ROOT / "oracle" / "_ref" / "libtgref.so"
+    if not path.exists():
+        return None
+    try:
+        from oracle import reference
+
+        return reference
+    except ImportError:
+        return None
+
+
+def _cpu_track(field, domain, seeds, rng_seed, threads):
+    """Track `seeds` on the CPU; returns (accepted steps, seconds, kind, description)."""
+    from oracle import oracle as O
+
+    n_steps = int(math.floor(MAX_LENGTH / SAVE_AT))
+    ref = _reference_lib()
+    if ref is not None:
+        t0 = time.perf_counter()
+        steps = ref.tractogram_steps(domain, field, "diffusion", STEP, GAMMA, NOISE, seeds, rng_seed, SAVE_AT,
+                                     n_steps, threads)
+        return steps, time.perf_counter() - t0, "reference", \
+            "reference OpenCL kernel source compiled as C++ (oracle/_ref), OpenMP over seeds"
+    case = O.Case(mask=domain.values, mask_inv_affine=domain.inverse_affine, field=field.values,
+                  field_inv_affine=field.inverse_affine, model=O.MODEL_SH, algorithm=O.ALGO_DIFFUSION,
+                  step_size=STEP, gamma=GAMMA, noise_variance=NOISE, rng_seed=rng_seed, save_at=SAVE_AT,
+                  n_steps=n_steps)
+    t0 = time.perf_counter()
+    _, _, steps = case.tractogram(seeds, n_threads=threads, return_steps=True)
+    return steps, time.perf_counter() - t0, "port", "plain-C oracle restating the reference kernel, OpenMP over seeds"
+
+
+def cpu_baseline(field, domain, seeds, threads=None):
+    """CPU throughput on a bounded sample (about 120 seeds per core) of the workload."""
+    threads = threads or os.cpu_count() or 1
+    n_sample = min(len(seeds), 120 * threads)
+    sample = np.ascontiguousarray(seeds[:n_sample])
+    steps, dt, kind, what = _cpu_track(field, domain, sample, 77, threads)
+    return {"value": steps / dt, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"first {n_sample} seeds of the timed batches ({steps} steps, {dt:.1f} s); {what}; "
+                      "pocl unavailable here"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import tractography_b200 as tg
+    from oracle import oracle as O
+    from tractography_b200 import synthetic
+
+    fod = synthetic.config1(seed=0)
+    field = tg.field.Image(fod)
+    mask = np.any(field.values != 0, axis=-1).astype(np.uint8)
+    domain = tg.domain.Image(tg.Nifti1Image(mask, fod.affine))
+    threads = os.cpu_count() or 1
+    per_step = max(8, 16 * threads)
+    inline, voxels, affine = tg.seeds.sparse_fod(fod)
+    np.random.seed(2024)
+    states = np.random.randint(4294967295, size=(per_step * (args.warmup + args.steps), 2)).astype(np.uint32)
+    seeds = O.seeds_from_fod(O.MODEL_SH, inline, voxels, affine, states, n_threads=threads)
+    algorithm = tg.algorithm.Diffusion(tg.local.RealSymmetricSphericalHarmonics(C), step_size=STEP, gamma=GAMMA,
+                                       noise_variance=NOISE, seed=1234)
+    total_steps, total_t = 0, 0.0
+    kind = what = ""
+    for i in range(args.warmup + args.steps):
+        chunk = np.ascontiguousarray(seeds[i * per_step:(i + 1) * per_step])
+        steps, dt, kind, what = _cpu_track(field, domain, chunk, algorithm.get_rng_seed(), threads)
+        if i >= args.warmup:
+            total_steps += steps
+            total_t += dt
+    value = total_steps / total_t if total_t > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_t / max(1, args.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator; no dataset)",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "batch_seeds": per_step,
+                   "note": "each step is a bounded sample of the workload on the host cores"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{per_step} seeds per step, {args.steps} timed steps; {what}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

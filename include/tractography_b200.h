@@ -1,0 +1,176 @@
+/*
+ * tractography_b200.h -- C ABI of the B200 streamline-tracking library
+ * (libtg_b200.so).
+ *
+ * The reference (cronos-inria/tractography) assembles OpenCL C from its
+ * plugin objects and launches one `tractogram` kernel per batch through
+ * PyOpenCL (tractography/tracking.py:22-178, tractography/opencl.py).  This
+ * library replaces that backend: the same kernel contract as compiled
+ * sm_100a code, with device-resident fields and domains, a persistent
+ * batched tracker and the standalone per-element kernels the reference
+ * exposes.  Plain C types only: pointers, sizes and POD structs.
+ *
+ * Conventions
+ *   - Every function returns a tg status code (TG_OK == 0).  On failure
+ *     tg_last_error() returns a message for the calling thread.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *   - Arrays are C-contiguous float32/uint32 in the layouts the reference
+ *     uses: seeds (n, 8) = (x, y, z, 1, dx, dy, dz, 0); points float4.
+ *   - Objects (tg_field, tg_domain, tg_tracker) are owned by the library
+ *     and released by their *_destroy function; per-call inputs and outputs
+ *     are owned by the caller.
+ *   - Threading: calls on different objects may run concurrently; calls on
+ *     one tg_tracker must be serialised by the caller.
+ */
+#ifndef TRACTOGRAPHY_B200_H
+#define TRACTOGRAPHY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TG_ABI_VERSION 1
+
+/* Status codes. */
+#define TG_OK 0
+#define TG_ERR_INVALID_ARGUMENT 1
+#define TG_ERR_CUDA 2
+#define TG_ERR_OUT_OF_MEMORY 3
+#define TG_ERR_UNSUPPORTED 4
+#define TG_ERR_POOL_EXHAUSTED 5
+
+/* Local models (tractography/local.py:74-262). */
+#define TG_MODEL_SH 0   /* RealSymmetricSphericalHarmonics, C <= 45 coefficients */
+#define TG_MODEL_DTI 1  /* DiffusionTensorImaging, 6 coefficients */
+
+/* Algorithms (tractography/algorithm.py:56-269). */
+#define TG_ALGO_TRANSPORT 0
+#define TG_ALGO_DIFFUSION 1
+
+/* Random streams. */
+#define TG_RNG_MWC64X 0  /* reference stream: rng_init(rng_seed, index in call), core.cl:180-245 */
+#define TG_RNG_PHILOX 1  /* counter-based Philox4x32-10 keyed by (philox_key, seed index, step) */
+
+typedef struct tg_field tg_field;
+typedef struct tg_domain tg_domain;
+typedef struct tg_tracker tg_tracker;
+
+/* Orientation-update parameters: the ALGORITHM_ARGS of algorithm.py:75,189
+ * plus the per-call rng_seed of tracking.py:164. */
+typedef struct {
+    int32_t algorithm;     /* TG_ALGO_* */
+    float step_size;       /* algorithm.step_size */
+    float gamma;           /* algorithm.gamma */
+    float noise_variance;  /* Diffusion only (algorithm.py:176) */
+    int32_t rng_mode;      /* TG_RNG_* */
+    uint32_t rng_seed;     /* MWC64X: seed of this call (Diffusion.get_rng_seed, algorithm.py:239-241) */
+    uint64_t philox_key;   /* Philox: stream key */
+    uint64_t seed_offset;  /* Philox: global index of seed 0 of this call */
+} tg_algorithm;
+
+/* Library information. */
+int tg_abi_version(void);
+const char* tg_status_string(int status);
+const char* tg_last_error(void);
+
+/* Device-resident image field.  Replaces field.Image.__init__ + get_args
+ * (tractography/field.py:54-69, 117-122), which re-uploaded the whole volume
+ * on every batch.  `values` is a host (nx, ny, nz, n_parameters) float32
+ * C-order array; `inverse_affine` is the row-major 4x4 world-to-voxel
+ * matrix in float32.  model = TG_MODEL_SH (any C <= 45) or TG_MODEL_DTI
+ * (C == 6). */
+int tg_field_create(int32_t model, const float* values, uint32_t nx, uint32_t ny, uint32_t nz,
+                    uint32_t n_parameters, const float inverse_affine[16], void* stream,
+                    tg_field** out);
+int tg_field_destroy(tg_field* field);
+
+/* Device-resident image domain.  Replaces domain.Image.__init__ + get_args
+ * (tractography/domain.py:275-311, 385-398).  `mask` is a host
+ * (nx, ny, nz) uint8 C-order array, nonzero = inside. */
+int tg_domain_create(const uint8_t* mask, uint32_t nx, uint32_t ny, uint32_t nz,
+                     const float inverse_affine[16], void* stream, tg_domain** out);
+int tg_domain_destroy(tg_domain* domain);
+
+/* The reference kernel contract (tracking.py:93-176): one launch over
+ * n_seeds device seeds; writes the dense (n_seeds, n_steps, 4) float32
+ * points and uint32 lengths to device memory exactly as the reference's
+ * `tractogram` kernel does.  Stream-ordered, does not synchronise. */
+int tg_tractogram(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
+                  const float* seeds, uint32_t n_seeds, float save_at, uint32_t n_steps,
+                  float* streamlines, uint32_t* lengths, void* stream);
+
+/* tg_tractogram with host buffers (tracking.py:152-176 including the
+ * uploads and read-backs); synchronises the stream. */
+int tg_tractogram_host(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
+                       const float* seeds, uint32_t n_seeds, float save_at, uint32_t n_steps,
+                       float* streamlines, uint32_t* lengths, void* stream);
+
+/* Persistent batched tracker (the tg.tractogram batch loop of
+ * tractography/__init__.py:524-539 as one device-scheduled launch).
+ * Seeds are split into batches of `batch_size`; batch b uses
+ * batch_rng_seeds[b] and stream ids 0..batch_size-1, which reproduces the
+ * per-batch MWC64X streams of the reference.  Points are packed, not dense.
+ * pool_points bounds the device point pool (0 = size on first use). */
+int tg_tracker_create(uint64_t pool_points, tg_tracker** out);
+int tg_tracker_destroy(tg_tracker* tracker);
+
+/* Track `n_seeds` seeds (device pointer, or host pointer when seeds_on_host
+ * != 0).  On return (the stream is synchronised) h_lengths[i] holds the
+ * point count of streamline i, h_offsets[i] the index of its first point in
+ * the tracker's packed point buffer, *total_points the buffer's size and
+ * *total_steps the number of accepted steps (loop iterations of
+ * tracking.py:121-147 that passed both checks).  batch_rng_seeds is a host
+ * array of ceil(n_seeds / batch_size) seeds. */
+int tg_tracker_run(tg_tracker* tracker, const tg_algorithm* algorithm, const tg_domain* domain,
+                   const tg_field* field, const float* seeds, int seeds_on_host, uint32_t n_seeds,
+                   uint32_t batch_size, const uint32_t* batch_rng_seeds, float save_at,
+                   uint32_t n_steps, uint32_t* h_lengths, uint64_t* h_offsets,
+                   uint64_t* total_points, uint64_t* total_steps, void* stream);
+
+/* Statistics of the last tg_tracker_run: device time of the tracking
+ * kernel launches (CUDA events on the run's stream), number of waves (more
+ * than one only when the point pool ran out) and number of kernel launches.
+ * No reference counterpart: instrumentation for the benchmark. */
+int tg_tracker_stats(const tg_tracker* tracker, float* kernel_ms, uint32_t* waves, uint32_t* launches);
+
+/* Copy points [first, first + count) of the packed (total_points, 3)
+ * float32 buffer of the last run to `dst` (host when dst_on_host != 0). */
+int tg_tracker_copy_points(tg_tracker* tracker, float* dst, uint64_t first, uint64_t count,
+                           int dst_on_host, void* stream);
+
+/* FOD seeding: seeds.cl:99-118 as launched by seeds.py:174-216.  `fod` is
+ * the device sparse (nnz, n_coefficients) array, `voxels` the device
+ * (nnz, 4) voxel indices with w = 1, `affine` the device voxel-to-world
+ * row-major 4x4, `states` the device (n_seeds, 2) MWC64X states drawn on the
+ * host.  Writes device (n_seeds, 8) seeds. */
+int tg_seeds_from_fod(int32_t model, uint32_t n_coefficients, const float* fod, const float* voxels,
+                      uint32_t nnz, const float* affine, const uint32_t* states, uint32_t n_seeds,
+                      float* seeds, void* stream);
+
+/* Per-element kernels of the reference's standalone entry points (device
+ * pointers; points/orientations are (n, 4) float32). */
+/* domain.contains, domain.py:433-491 */
+int tg_domain_contains(const tg_domain* domain, const float* points, uint32_t n, uint8_t* out,
+                       void* stream);
+/* field.evaluate, field.py:144-197: out (n, C) */
+int tg_field_evaluate(const tg_field* field, const float* points, uint32_t n, float* out, void* stream);
+/* local.evaluate, local.py:285-363: out (n, 3) = value, d/dtheta, (d/dphi)/sin(theta) */
+int tg_local_evaluate(int32_t model, uint32_t n_parameters, const float* parameters,
+                      const float* orientations, uint32_t n, float* out, void* stream);
+/* algorithm.update_orientation, algorithm.py:701-790: out (n, 4) */
+int tg_update_orientation(int32_t model, uint32_t n_parameters, const tg_algorithm* algorithm,
+                          const float* parameters, const float* orientations, uint32_t n, float* out,
+                          void* stream);
+/* randus / randis test streams, core.cl:218-238 (which: 0 randu, 1 randn,
+ * 2 randi below `max`), from the raw MWC64X state (s0, s1). */
+int tg_rng_stream(int32_t which, uint32_t s0, uint32_t s1, uint32_t n, uint32_t max, void* out,
+                  void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TRACTOGRAPHY_B200_H */

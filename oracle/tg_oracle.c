@@ -1,0 +1,632 @@
+/*
+ * tg_oracle.c -- CPU oracle (test infrastructure only; see tg_oracle.h).
+ *
+ * Restates, in plain C, the reference's tracking kernel
+ * (tractography/tracking.py:93-149) with its plugins: image domain
+ * (domain.py:358-382), image field (field.py:88-114), spherical-harmonic and
+ * tensor local models (local.py:91-120, 212-230; spharm.cl:216-413;
+ * core.cl:111-120, 142-153), Transport and Diffusion updates
+ * (algorithm.py:83-112, 198-228; core.cl:101-109), the MWC64X stream
+ * (core.cl:180-245) and FOD seeding (seeds.cl:12-118, seeds.py:174-216).
+ *
+ * Build: gcc -O2 -std=c99 -ffp-contract=off -fopenmp (see oracle/Makefile).
+ */
+#include "tg_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "tg_fmath.h"
+#include "tg_sh_table.h"
+
+#define N_DIRECTIONS 1000
+#define SOFTMAX_SCALE 100.0f
+
+/* OpenCL max()/min() on floats (x < y ? y : x), core to the reference's
+ * max(value, 1e-6f) and max(value, 0.0f). */
+static float cl_maxf(float x, float y) { return (x < y) ? y : x; }
+
+/* ------------------------------------------------------------------ */
+/* RNG: core.cl:180-245                                                */
+/* ------------------------------------------------------------------ */
+
+static uint32_t mwc64x(uint32_t s[2])
+{
+    const uint32_t A = 4294883355u;                 /* core.cl:182 */
+    uint32_t x = s[0], c = s[1];
+    const uint32_t res = x ^ c;
+    const uint32_t hi = (uint32_t)(((uint64_t)x * A) >> 32);
+    x = x * A + c;
+    c = hi + (x < c);
+    s[0] = x;
+    s[1] = c;
+    return res;
+}
+
+static uint32_t rng_mix32(uint32_t v)               /* core.cl:193-201 */
+{
+    v ^= v >> 16;
+    v *= 0x7feb352du;
+    v ^= v >> 15;
+    v *= 0x846ca68bu;
+    v ^= v >> 16;
+    return v;
+}
+
+void tgo_rng_init(uint32_t seed, uint32_t id, uint32_t s[2])   /* core.cl:203-208 */
+{
+    uint32_t x = rng_mix32(seed ^ (id + 0x9e3779b9u));
+    if (x < 1u) x = 1u;
+    s[0] = x;
+    s[1] = rng_mix32(seed + id * 0x85ebca6bu) % 4294883355u;
+}
+
+static float randu(uint32_t s[2])                    /* core.cl:212-214 */
+{
+    return (float)(mwc64x(s) >> 8) * 0x1p-24f;
+}
+
+static uint32_t randi(uint32_t s[2], uint32_t max)   /* core.cl:227-229 */
+{
+    return (uint32_t)(randu(s) * (float)max);
+}
+
+static float randn(uint32_t s[2])                    /* core.cl:240-245 */
+{
+    float n = randu(s);
+    while (n <= 0.0f) n = randu(s);
+    const float radius = sqrtf(-2.0f * tgm_logf(n));
+    return radius * tgm_cosf(TGM_TWO_PI * randu(s));
+}
+
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter-based stream
+ * used by the optional keyed mode (north-star item (b)). */
+void tgo_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int round = 0; round < 10; ++round) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* Two standard normals for (seed index, step) under a key: Box-Muller on
+ * u1 = ((w0 >> 8) + 1) 2^-24 in (0, 1] and u2 = (w1 >> 8) 2^-24. */
+static void philox_normal2(uint64_t key, uint64_t index, uint32_t step, float* n1, float* n2)
+{
+    const uint32_t ctr[4] = {(uint32_t)index, (uint32_t)(index >> 32), step, 0x5eedu};
+    const uint32_t k[2] = {(uint32_t)key, (uint32_t)(key >> 32)};
+    uint32_t w[4];
+    tgo_philox(ctr, k, w);
+    const float u1 = (float)((w[0] >> 8) + 1u) * 0x1p-24f;
+    const float u2 = (float)(w[1] >> 8) * 0x1p-24f;
+    const float radius = sqrtf(-2.0f * tgm_logf(u1));
+    float s, c;
+    tgm_sincosf(TGM_TWO_PI * u2, &s, &c);
+    *n1 = radius * c;
+    *n2 = radius * s;
+}
+
+/* ------------------------------------------------------------------ */
+/* Geometry: core.cl:142-153 (cart2sph) expressed as the frame        */
+/* cos/sin of colatitude and azimuth.                                 */
+/* ------------------------------------------------------------------ */
+
+typedef struct { float ct, st, cp, sp; } frame_t;
+
+static frame_t frame_of(float x, float y, float z)
+{
+    frame_t f;
+    const float rho2 = fmaf(y, y, x * x);
+    const float r2 = fmaf(z, z, rho2);
+    const float r = sqrtf(r2);
+    if (r <= 0.0f) {                                 /* core.cl:144-146 */
+        f.ct = 1.0f; f.st = 0.0f; f.cp = 1.0f; f.sp = 0.0f;
+        return f;
+    }
+    const float ir = 1.0f / r;
+    f.ct = fminf(fmaxf(z * ir, -1.0f), 1.0f);        /* core.cl:151 clamp */
+    const float rho = sqrtf(rho2);
+    f.st = fminf(rho * ir, 1.0f);
+    if (rho > 0.0f) {
+        const float irho = 1.0f / rho;
+        f.cp = x * irho;
+        f.sp = y * irho;
+    } else {                                         /* atan2(0, 0) = 0 */
+        f.cp = 1.0f;
+        f.sp = 0.0f;
+    }
+    return f;
+}
+
+/* x.row of a row-major 4x4 matrix (used for both the inverse affines of
+ * domain.py:362-366 / field.py:92-96 and apply_affine of core.cl:164-170). */
+static float dot4(const float* a, float x, float y, float z, float w)
+{
+    return fmaf(a[3], w, fmaf(a[2], z, fmaf(a[1], y, a[0] * x)));
+}
+
+/* ------------------------------------------------------------------ */
+/* Local models                                                        */
+/* ------------------------------------------------------------------ */
+
+typedef struct { float value, dtheta, dphi; } model_value_t;
+
+static int lmax_for(uint32_t n_params)
+{
+    int l = 0;
+    while ((uint32_t)((l + 1) * (l + 2) / 2) < n_params) l += 2;
+    return l;
+}
+
+static float horner_u(const float* a, int n, float u)
+{
+    float h = a[n - 1];
+    for (int j = n - 2; j >= 0; --j) h = fmaf(h, u, a[j]);
+    return h;
+}
+
+/* Sum of c_i Y_i, d/dtheta and (d/dphi)/sin(theta) for l <= lmax; the
+ * coefficient vector c is zero-padded to the full band. */
+static model_value_t sh_raw(const float* c, int lmax, frame_t f)
+{
+    const float ct = f.ct, st = f.st, cp = f.cp, sp = f.sp;
+    const float u = ct * ct;
+    const float tc = cp + cp;
+    float cm[TG_SH_LMAX + 1], sm[TG_SH_LMAX + 1], stp[TG_SH_LMAX + 2];
+    cm[0] = 1.0f; sm[0] = 0.0f;
+    cm[1] = cp; sm[1] = sp;
+    for (int m = 2; m <= lmax; ++m) {
+        cm[m] = fmaf(tc, cm[m - 1], -cm[m - 2]);
+        sm[m] = fmaf(tc, sm[m - 1], -sm[m - 2]);
+    }
+    stp[0] = 1.0f;
+    for (int k = 1; k <= lmax + 1; ++k) stp[k] = stp[k - 1] * st;
+
+    model_value_t r = {0.0f, 0.0f, 0.0f};
+    for (int m = 0; m <= lmax; ++m) {
+        float A = 0.0f, B = 0.0f, Ap = 0.0f, Bp = 0.0f;
+        int any = 0;
+        for (int k = 0; k < TG_SH_NPAIRS; ++k) {
+            const int* e = TG_SH_PAIRS[k];
+            const int l = e[0];
+            if (e[1] != m || l > lmax) continue;
+            any = 1;
+            const int ip = l * (l + 1) / 2 + m;
+            const int im = l * (l + 1) / 2 - m;
+            float R = horner_u(TG_SH_COEF + e[3], e[4], u);
+            if (e[2]) R = R * ct;
+            A = fmaf(c[ip], R, A);
+            if (m > 0) B = fmaf(c[im], R, B);
+            if (l > m) {
+                float Rp = horner_u(TG_SH_COEF + e[5], e[6], u);
+                if (!e[2]) Rp = Rp * ct;
+                Ap = fmaf(c[ip], Rp, Ap);
+                if (m > 0) Bp = fmaf(c[im], Rp, Bp);
+            }
+        }
+        if (!any) continue;
+        if (m == 0) {
+            r.value = r.value + A;
+            r.dtheta = fmaf(-stp[1], Ap, r.dtheta);
+        } else {
+            const float F = fmaf(B, sm[m], A * cm[m]);
+            const float Fp = fmaf(Bp, sm[m], Ap * cm[m]);
+            const float G = fmaf(-A, sm[m], B * cm[m]);
+            r.value = fmaf(stp[m], F, r.value);
+            const float mw = (float)m * stp[m - 1];
+            const float wct = mw * ct;
+            r.dtheta = fmaf(wct, F, r.dtheta);
+            r.dtheta = fmaf(-stp[m + 1], Fp, r.dtheta);
+            r.dphi = fmaf(mw, G, r.dphi);
+        }
+    }
+    return r;
+}
+
+/* core.cl:111-120 */
+static float softmax(float x, float k)
+{
+    if (x * k < 30.0f) return tgm_logf(1.0f + tgm_expf(k * x)) / k;
+    return x;
+}
+
+static float dsoftmax(float x, float k)
+{
+    return 1.0f / (1.0f + tgm_expf(-k * x));
+}
+
+/* local.py:91-120 */
+static model_value_t sh_model(const float* params, uint32_t n_params, frame_t f)
+{
+    float c[48];
+    const int lmax = lmax_for(n_params);
+    const int full = (lmax + 1) * (lmax + 2) / 2;
+    for (int i = 0; i < full; ++i) c[i] = (uint32_t)i < n_params ? params[i] : 0.0f;
+    model_value_t r = sh_raw(c, lmax, f);
+    const float d = dsoftmax(r.value, SOFTMAX_SCALE);
+    r.value = softmax(r.value, SOFTMAX_SCALE);
+    r.dtheta = r.dtheta * d;
+    r.dphi = r.dphi * d;
+    return r;
+}
+
+/* local.py:212-230 (orientation used as given, angles from its direction). */
+static model_value_t dti_model(const float* m, float x, float y, float z, frame_t f)
+{
+    const float dux = fmaf(m[4], z, fmaf(m[3], y, m[0] * x));
+    const float duy = fmaf(m[5], z, fmaf(m[1], y, m[3] * x));
+    const float duz = fmaf(m[2], z, fmaf(m[5], y, m[4] * x));
+    model_value_t r;
+    r.value = fmaf(z, duz, fmaf(y, duy, x * dux));
+    const float etx = f.ct * f.cp, ety = f.ct * f.sp, etz = -f.st;
+    r.dtheta = 2.0f * fmaf(duz, etz, fmaf(duy, ety, dux * etx));
+    r.dphi = 2.0f * fmaf(duy, f.cp, dux * (-f.sp));
+    return r;
+}
+
+static model_value_t model_eval(int32_t model, const float* params, uint32_t n_params,
+                                float x, float y, float z, frame_t f)
+{
+    if (model == TGO_MODEL_DTI) return dti_model(params, x, y, z, f);
+    return sh_model(params, n_params, f);
+}
+
+/* ------------------------------------------------------------------ */
+/* Algorithms: algorithm.py:83-112 (Transport), 198-228 (Diffusion)   */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    uint32_t mwc[2];
+    uint64_t index;
+    uint32_t step;
+} rng_t;
+
+static void exps2(float o[3], const float t[3])      /* core.cl:101-109 */
+{
+    const float n = sqrtf(fmaf(t[2], t[2], fmaf(t[1], t[1], t[0] * t[0])));
+    if (n <= 0.0f) return;
+    float s, c;
+    tgm_sincosf(n, &s, &c);
+    const float k = s / n;
+    o[0] = fmaf(t[0], k, c * o[0]);
+    o[1] = fmaf(t[1], k, c * o[1]);
+    o[2] = fmaf(t[2], k, c * o[2]);
+}
+
+static void update_orientation(const tgo_problem* p, const float* params, uint32_t n_params,
+                               float o[3], rng_t* rng)
+{
+    const frame_t f = frame_of(o[0], o[1], o[2]);
+    const model_value_t mv = model_eval(p->model, params, n_params, o[0], o[1], o[2], f);
+    const float etx = f.ct * f.cp, ety = f.ct * f.sp, etz = -f.st;
+    const float epx = -f.sp, epy = f.cp;
+    const float inv = 1.0f / cl_maxf(mv.value, 1e-6f);
+    const float gx = fmaf(mv.dphi, epx, mv.dtheta * etx);
+    const float gy = fmaf(mv.dphi, epy, mv.dtheta * ety);
+    const float gz = mv.dtheta * etz;
+    const float dx = gx * inv, dy = gy * inv, dz = gz * inv;
+    const float scale_drift = p->gamma * p->step_size;
+    float t[3];
+    if (p->algorithm == TGO_ALGO_TRANSPORT) {
+        t[0] = scale_drift * dx;
+        t[1] = scale_drift * dy;
+        t[2] = scale_drift * dz;
+    } else {
+        float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+        if (p->noise_variance > 0.0f) {
+            float n1, n2;
+            if (p->rng_mode == TGO_RNG_MWC64X) {
+                n1 = randn(rng->mwc);                 /* first draw scales e_theta */
+                n2 = randn(rng->mwc);
+            } else {
+                philox_normal2(p->philox_key, rng->index, rng->step, &n1, &n2);
+            }
+            nx = fmaf(n2, epx, n1 * etx);
+            ny = fmaf(n2, epy, n1 * ety);
+            nz = n1 * etz;
+        }
+        const float scale_noise = sqrtf(p->noise_variance * p->gamma * p->step_size);
+        t[0] = fmaf(scale_noise, nx, scale_drift * dx);
+        t[1] = fmaf(scale_noise, ny, scale_drift * dy);
+        t[2] = fmaf(scale_noise, nz, scale_drift * dz);
+    }
+    exps2(o, t);
+    rng->step += 1u;
+}
+
+/* ------------------------------------------------------------------ */
+/* Domain and field                                                    */
+/* ------------------------------------------------------------------ */
+
+/* domain.py:358-382: nearest voxel by floor(v + 0.5), half-open cells. */
+static int domain_contains(const tgo_problem* p, float x, float y, float z)
+{
+    int32_t idx[3];
+    for (int i = 0; i < 3; ++i) {
+        const float v = floorf(dot4(p->mask_inv_affine + 4 * i, x, y, z, 1.0f) + 0.5f);
+        if (!(v >= 0.0f && v < (float)p->mask_dims[i])) return 0;
+        idx[i] = (int32_t)v;
+    }
+    const size_t k = ((size_t)idx[0] * p->mask_dims[1] + (size_t)idx[1]) * p->mask_dims[2] + (size_t)idx[2];
+    return p->mask[k] != 0;
+}
+
+/* field.py:88-114: nearest voxel by rint (ties to even); 0 when outside. */
+static const float* field_voxel(const tgo_problem* p, float x, float y, float z)
+{
+    int32_t idx[3];
+    for (int i = 0; i < 3; ++i) {
+        const float v = rintf(dot4(p->field_inv_affine + 4 * i, x, y, z, 1.0f));
+        if (!(v >= 0.0f && v < (float)p->field_dims[i])) return NULL;
+        idx[i] = (int32_t)v;
+    }
+    const size_t k = ((size_t)idx[0] * p->field_dims[1] + (size_t)idx[1]) * p->field_dims[2] + (size_t)idx[2];
+    return p->field + k * p->field_dims[3];
+}
+
+/* ------------------------------------------------------------------ */
+/* Tracking loop: tracking.py:105-148                                  */
+/* ------------------------------------------------------------------ */
+
+static uint32_t track_one(const tgo_problem* p, const float* seed, uint32_t gid, float* out,
+                          uint64_t* steps)
+{
+    const uint32_t n_steps = p->n_steps;
+    const uint32_t C = p->field_dims[3];
+    float pos[3] = {seed[0], seed[1], seed[2]};
+    float o[3] = {seed[4], seed[5], seed[6]};
+    rng_t rng;
+    tgo_rng_init(p->rng_seed, gid, rng.mwc);
+    rng.index = p->seed_offset + gid;
+    rng.step = 0u;
+    out[0] = seed[0]; out[1] = seed[1]; out[2] = seed[2]; out[3] = seed[3];
+    uint32_t n = 1;
+    float time = 0.0f;
+    while (n < n_steps) {
+        if (!domain_contains(p, pos[0], pos[1], pos[2])) break;
+        const float* c = field_voxel(p, pos[0], pos[1], pos[2]);
+        if (!c) break;
+        update_orientation(p, c, C, o, &rng);
+        *steps += 1;
+        pos[0] = fmaf(p->step_size, o[0], pos[0]);
+        pos[1] = fmaf(p->step_size, o[1], pos[1]);
+        pos[2] = fmaf(p->step_size, o[2], pos[2]);
+        time = time + p->step_size;
+        if (time >= p->save_at) {
+            time = time - p->save_at;
+            float* q = out + 4 * (size_t)n;
+            q[0] = fmaf(-time, o[0], pos[0]);
+            q[1] = fmaf(-time, o[1], pos[1]);
+            q[2] = fmaf(-time, o[2], pos[2]);
+            q[3] = 1.0f;
+            n++;
+        }
+    }
+    return n;
+}
+
+uint64_t tgo_tractogram(const tgo_problem* p, const float* seeds, uint32_t n_seeds,
+                        float* streamlines, uint32_t* lengths, int n_threads)
+{
+    if (p->n_steps == 0) {
+        for (uint32_t i = 0; i < n_seeds; ++i) lengths[i] = 0;
+        return 0;
+    }
+    uint64_t total = 0;
+    long i;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : total) num_threads(n_threads > 0 ? n_threads : 1)
+    for (i = 0; i < (long)n_seeds; ++i) {
+        float* out = streamlines + (size_t)i * p->n_steps * 4;
+        uint64_t steps = 0;
+        lengths[i] = track_one(p, seeds + 8 * (size_t)i, (uint32_t)i, out, &steps);
+        total += steps;
+    }
+    return total;
+}
+
+void tgo_contains(const tgo_problem* p, const float* points, uint32_t n, uint8_t* out)
+{
+    for (uint32_t i = 0; i < n; ++i)
+        out[i] = (uint8_t)domain_contains(p, points[4 * i], points[4 * i + 1], points[4 * i + 2]);
+}
+
+void tgo_field_evaluate(const tgo_problem* p, const float* points, uint32_t n, float* out)
+{
+    const uint32_t C = p->field_dims[3];
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* c = field_voxel(p, points[4 * i], points[4 * i + 1], points[4 * i + 2]);
+        for (uint32_t j = 0; j < C; ++j) out[(size_t)i * C + j] = c ? c[j] : 0.0f;
+    }
+}
+
+void tgo_local_evaluate(int32_t model, uint32_t n_params, const float* params,
+                        const float* orientations, uint32_t n, float* out)
+{
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* o = orientations + 4 * (size_t)i;
+        const frame_t f = frame_of(o[0], o[1], o[2]);
+        const model_value_t r = model_eval(model, params + (size_t)i * n_params, n_params, o[0], o[1], o[2], f);
+        out[3 * i] = r.value;
+        out[3 * i + 1] = r.dtheta;
+        out[3 * i + 2] = r.dphi;
+    }
+}
+
+void tgo_update_orientation(const tgo_problem* p, uint32_t n_params, const float* params,
+                            const float* orientations, uint32_t n, float* out)
+{
+    for (uint32_t i = 0; i < n; ++i) {
+        rng_t rng;
+        tgo_rng_init(p->rng_seed, i, rng.mwc);
+        rng.index = p->seed_offset + i;
+        rng.step = 0u;
+        float o[3] = {orientations[4 * i], orientations[4 * i + 1], orientations[4 * i + 2]};
+        update_orientation(p, params + (size_t)i * n_params, n_params, o, &rng);
+        out[4 * i] = o[0]; out[4 * i + 1] = o[1]; out[4 * i + 2] = o[2]; out[4 * i + 3] = 0.0f;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* FOD seeding: seeds.cl:12-118                                        */
+/* ------------------------------------------------------------------ */
+
+/* seeds.cl:12-25: n-th of n_points Fibonacci-lattice directions. */
+static void fibonacci(uint32_t n, uint32_t n_points, float d[3])
+{
+    const float phi = (sqrtf(5.0f) + 1.0f) * 0.5f;
+    const float golden_angle = TGM_TWO_PI / phi;
+    const float theta = (float)n * golden_angle;
+    const float z = 1.0f - (2.0f * (float)n / (float)(n_points - 1));
+    const float radius = sqrtf(fmaf(-z, z, 1.0f));
+    float s, c;
+    tgm_sincosf(theta, &s, &c);
+    d[0] = radius * c;
+    d[1] = radius * s;
+    d[2] = z;
+}
+
+/* Real SH basis Y_i (i < (lmax+1)(lmax+2)/2) at one direction, the
+ * value-only companion of sh_raw: Y = R * st^m * trig(m phi). */
+static void sh_basis(int lmax, frame_t f, float* Y)
+{
+    const float ct = f.ct, st = f.st, cp = f.cp, sp = f.sp;
+    const float u = ct * ct;
+    const float tc = cp + cp;
+    float cm[TG_SH_LMAX + 1], sm[TG_SH_LMAX + 1], stp[TG_SH_LMAX + 1];
+    cm[0] = 1.0f; sm[0] = 0.0f; cm[1] = cp; sm[1] = sp;
+    for (int m = 2; m <= lmax; ++m) {
+        cm[m] = fmaf(tc, cm[m - 1], -cm[m - 2]);
+        sm[m] = fmaf(tc, sm[m - 1], -sm[m - 2]);
+    }
+    stp[0] = 1.0f;
+    for (int k = 1; k <= lmax; ++k) stp[k] = stp[k - 1] * st;
+    for (int k = 0; k < TG_SH_NPAIRS; ++k) {
+        const int* e = TG_SH_PAIRS[k];
+        const int l = e[0], m = e[1];
+        if (l > lmax) continue;
+        float R = horner_u(TG_SH_COEF + e[3], e[4], u);
+        if (e[2]) R = R * ct;
+        const int ip = l * (l + 1) / 2 + m;
+        if (m == 0) {
+            Y[ip] = R;
+        } else {
+            const float P = R * stp[m];
+            Y[ip] = P * cm[m];
+            Y[l * (l + 1) / 2 - m] = P * sm[m];
+        }
+    }
+}
+
+typedef struct {
+    float dir[N_DIRECTIONS][3];
+    float Y[N_DIRECTIONS][48];
+} fib_table_t;
+
+static float fod_value(int32_t model, const float* c, uint32_t C, const fib_table_t* t, int i)
+{
+    if (model == TGO_MODEL_DTI) {
+        const float* d = t->dir[i];
+        const frame_t f = frame_of(d[0], d[1], d[2]);
+        return dti_model(c, d[0], d[1], d[2], f).value;
+    }
+    float raw = 0.0f;
+    for (uint32_t j = 0; j < C; ++j) raw = fmaf(c[j], t->Y[i][j], raw);
+    return softmax(raw, SOFTMAX_SCALE);
+}
+
+void tgo_seeds_from_fod(int32_t model, uint32_t C, const float* fod,
+                        const float* voxels, uint32_t nnz, const float affine[16],
+                        const uint32_t* states, uint32_t n_seeds, float* seeds,
+                        int n_threads)
+{
+    fib_table_t* t = (fib_table_t*)malloc(sizeof(fib_table_t));
+    const int lmax = lmax_for(C);
+    for (int i = 0; i < N_DIRECTIONS; ++i) {
+        fibonacci((uint32_t)i, N_DIRECTIONS, t->dir[i]);
+        if (model == TGO_MODEL_SH) {
+            const frame_t f = frame_of(t->dir[i][0], t->dir[i][1], t->dir[i][2]);
+            sh_basis(lmax, f, t->Y[i]);
+        }
+    }
+    long g;
+#pragma omp parallel for schedule(static) num_threads(n_threads > 0 ? n_threads : 1)
+    for (g = 0; g < (long)n_seeds; ++g) {
+        uint32_t s[2] = {states[2 * g], states[2 * g + 1]};
+        uint32_t vi = randi(s, nnz);                  /* seeds.cl:89 */
+        if (vi >= nnz) vi = nnz - 1;
+        const float* v = voxels + 4 * (size_t)vi;
+        float vx = v[0], vy = v[1], vz = v[2], vw = v[3];
+        vx = vx + (randu(s) - 0.5f);                 /* seeds.cl:94, x then y then z */
+        vy = vy + (randu(s) - 0.5f);
+        vz = vz + (randu(s) - 0.5f);
+        const float* c = fod + (size_t)vi * C;
+        float sum = 0.0f;                            /* seeds.cl:29-35 */
+        for (int i = 0; i < N_DIRECTIONS; ++i) sum = sum + cl_maxf(fod_value(model, c, C, t, i), 0.0f);
+        const float threshold = randu(s) * sum;      /* seeds.cl:38 */
+        float cs = 0.0f;
+        int selected = N_DIRECTIONS;
+        for (int i = 0; i < N_DIRECTIONS; ++i) {
+            cs = cs + cl_maxf(fod_value(model, c, C, t, i), 0.0f);
+            if (selected == N_DIRECTIONS && cs > threshold) selected = i;
+        }
+        float* out = seeds + 8 * (size_t)g;
+        out[0] = dot4(affine + 0, vx, vy, vz, vw);   /* seeds.cl:105, apply_affine */
+        out[1] = dot4(affine + 4, vx, vy, vz, vw);
+        out[2] = dot4(affine + 8, vx, vy, vz, vw);
+        out[3] = dot4(affine + 12, vx, vy, vz, vw);
+        if (selected < N_DIRECTIONS) {
+            out[4] = t->dir[selected][0]; out[5] = t->dir[selected][1]; out[6] = t->dir[selected][2];
+        } else {
+            out[4] = 0.0f; out[5] = 0.0f; out[6] = 1.0f;
+        }
+        out[7] = 0.0f;
+    }
+    free(t);
+}
+
+/* ------------------------------------------------------------------ */
+/* Streams for tests (core.cl:218-238)                                 */
+/* ------------------------------------------------------------------ */
+
+void tgo_randu_stream(uint32_t s0, uint32_t s1, uint32_t n, float* out)
+{
+    uint32_t s[2] = {s0, s1};
+    for (uint32_t i = 0; i < n; ++i) out[i] = randu(s);
+}
+
+void tgo_randn_stream(uint32_t s0, uint32_t s1, uint32_t n, float* out)
+{
+    uint32_t s[2] = {s0, s1};
+    for (uint32_t i = 0; i < n; ++i) out[i] = randn(s);
+}
+
+void tgo_randi_stream(uint32_t s0, uint32_t s1, uint32_t n, uint32_t max, uint32_t* out)
+{
+    uint32_t s[2] = {s0, s1};
+    for (uint32_t i = 0; i < n; ++i) out[i] = randi(s, max);
+}
+
+void tgo_math(int which, const float* x, uint32_t n, float* out)
+{
+    for (uint32_t i = 0; i < n; ++i) {
+        switch (which) {
+        case 0: out[i] = tgm_sinf(x[i]); break;
+        case 1: out[i] = tgm_cosf(x[i]); break;
+        case 2: out[i] = tgm_expf(x[i]); break;
+        case 3: out[i] = tgm_logf(x[i]); break;
+        default: out[i] = x[i]; break;
+        }
+    }
+}

@@ -1,0 +1,95 @@
+/*
+ * tg_oracle.h -- CPU oracle for the streamline-tracking path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the
+ * reference's OpenCL tracking kernel and its plugins, used by the tests, by
+ * the smoke check and by the benchmark's CPU-baseline leg to check the CUDA
+ * path.  Nothing in the product links or calls it.
+ *
+ * Arithmetic contract: every float operation below is an IEEE-754 binary32
+ * operation in a fixed order (explicit fmaf, no contraction, transcendentals
+ * from tg_fmath.h), the same contract the CUDA kernels follow, so the two
+ * agree bit for bit.  Against the reference itself (whose transcendentals
+ * come from the OpenCL platform) agreement is to float tolerance.
+ */
+#ifndef TG_ORACLE_H
+#define TG_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { TGO_MODEL_SH = 0, TGO_MODEL_DTI = 1 };
+enum { TGO_ALGO_TRANSPORT = 0, TGO_ALGO_DIFFUSION = 1 };
+enum { TGO_RNG_MWC64X = 0, TGO_RNG_PHILOX = 1 };
+
+typedef struct {
+    /* domain (domain.py:350-356): int32 mask, dims, inverse affine rows */
+    const int32_t* mask;
+    uint32_t mask_dims[3];
+    float mask_inv_affine[16];
+    /* field (field.py:82-86): float32 (X, Y, Z, C), dims, inverse affine */
+    const float* field;
+    uint32_t field_dims[4];
+    float field_inv_affine[16];
+    /* local model and algorithm (local.py:74-230, algorithm.py:56-228) */
+    int32_t model;
+    int32_t algorithm;
+    float step_size;
+    float gamma;
+    float noise_variance;
+    /* random stream: MWC64X seeded by rng_init(rng_seed, index within the
+     * call) as the reference does, or Philox4x32-10 keyed by philox_key and
+     * counted by (seed_offset + index, step). */
+    int32_t rng_mode;
+    uint32_t rng_seed;
+    uint64_t philox_key;
+    uint64_t seed_offset;
+    /* output */
+    float save_at;
+    uint32_t n_steps;
+} tgo_problem;
+
+/* tracking.py:93-149: dense (n_seeds, n_steps, 4) points and lengths.
+ * Returns the number of accepted steps (loop iterations that passed both the
+ * domain and the field check). */
+uint64_t tgo_tractogram(const tgo_problem* p, const float* seeds, uint32_t n_seeds,
+                        float* streamlines, uint32_t* lengths, int n_threads);
+
+/* domain.py:358-382 for n points (x, y, z, w) -> 0/1. */
+void tgo_contains(const tgo_problem* p, const float* points, uint32_t n, uint8_t* out);
+
+/* field.py:88-114 for n points -> (n, C) coefficients, zero outside. */
+void tgo_field_evaluate(const tgo_problem* p, const float* points, uint32_t n, float* out);
+
+/* local.py:91-120, 212-230: (n, 3) value, d/dtheta, (d/dphi)/sin(theta). */
+void tgo_local_evaluate(int32_t model, uint32_t n_params, const float* params,
+                        const float* orientations, uint32_t n, float* out);
+
+/* algorithm.py:738-759: one orientation update per row, RNG stream per row. */
+void tgo_update_orientation(const tgo_problem* p, uint32_t n_params, const float* params,
+                            const float* orientations, uint32_t n, float* out);
+
+/* seeds.cl:68-118 + seeds.py:174-216: seeds (n, 8) from a sparse FOD. */
+void tgo_seeds_from_fod(int32_t model, uint32_t n_coefficients, const float* fod,
+                        const float* voxels, uint32_t nnz, const float affine[16],
+                        const uint32_t* states, uint32_t n_seeds, float* seeds,
+                        int n_threads);
+
+/* core.cl:180-245 primitives. */
+void tgo_rng_init(uint32_t seed, uint32_t stream_id, uint32_t state[2]);
+void tgo_randu_stream(uint32_t s0, uint32_t s1, uint32_t n, float* out);
+void tgo_randn_stream(uint32_t s0, uint32_t s1, uint32_t n, float* out);
+void tgo_randi_stream(uint32_t s0, uint32_t s1, uint32_t n, uint32_t max, uint32_t* out);
+void tgo_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* Shared math layer, exposed so tests can measure its accuracy. */
+void tgo_math(int which, const float* x, uint32_t n, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

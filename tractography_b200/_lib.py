@@ -1,0 +1,137 @@
+"""ctypes binding of ``libtg_b200.so`` (the C ABI of include/tractography_b200.h).
+
+The library is built in-tree by ``__graft_entry__.build()`` (or ``make -C
+tractography_b200/csrc``).  There is no CPU fallback: if the library is
+missing, every GPU entry point raises ``RuntimeError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libtg_b200.so"
+
+TG_OK = 0
+TG_ERR_INVALID_ARGUMENT = 1
+TG_ERR_CUDA = 2
+TG_ERR_OUT_OF_MEMORY = 3
+TG_ERR_UNSUPPORTED = 4
+TG_ERR_POOL_EXHAUSTED = 5
+
+MODEL_SH = 0
+MODEL_DTI = 1
+ALGO_TRANSPORT = 0
+ALGO_DIFFUSION = 1
+RNG_MWC64X = 0
+RNG_PHILOX = 1
+
+# Every symbol the header declares; tests check the library exports them.
+EXPORTS = (
+    "tg_abi_version",
+    "tg_status_string",
+    "tg_last_error",
+    "tg_field_create",
+    "tg_field_destroy",
+    "tg_domain_create",
+    "tg_domain_destroy",
+    "tg_tractogram",
+    "tg_tractogram_host",
+    "tg_tracker_create",
+    "tg_tracker_destroy",
+    "tg_tracker_run",
+    "tg_tracker_stats",
+    "tg_tracker_copy_points",
+    "tg_seeds_from_fod",
+    "tg_domain_contains",
+    "tg_field_evaluate",
+    "tg_local_evaluate",
+    "tg_update_orientation",
+    "tg_rng_stream",
+)
+
+
+class Algorithm(ctypes.Structure):
+    """Mirror of ``tg_algorithm``."""
+
+    _fields_ = [
+        ("algorithm", ctypes.c_int32),
+        ("step_size", ctypes.c_float),
+        ("gamma", ctypes.c_float),
+        ("noise_variance", ctypes.c_float),
+        ("rng_mode", ctypes.c_int32),
+        ("rng_seed", ctypes.c_uint32),
+        ("philox_key", ctypes.c_uint64),
+        ("seed_offset", ctypes.c_uint64),
+    ]
+
+
+class TgError(RuntimeError):
+    """A failed library call; ``status`` holds the tg status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the library (once) and declare the signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"the CUDA library {LIB_PATH} is not built; run "
+            "`python -c 'import __graft_entry__ as g; g.build()'` or "
+            "`make -C tractography_b200/csrc`"
+        )
+    lib = ctypes.CDLL(str(LIB_PATH))
+    P = ctypes.c_void_p
+    U32, I32, U64, F = ctypes.c_uint32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_float
+    AP = ctypes.POINTER(Algorithm)
+    sig = {
+        "tg_abi_version": ([], ctypes.c_int),
+        "tg_status_string": ([ctypes.c_int], ctypes.c_char_p),
+        "tg_last_error": ([], ctypes.c_char_p),
+        "tg_field_create": ([I32, P, U32, U32, U32, U32, P, P, ctypes.POINTER(P)], ctypes.c_int),
+        "tg_field_destroy": ([P], ctypes.c_int),
+        "tg_domain_create": ([P, U32, U32, U32, P, P, ctypes.POINTER(P)], ctypes.c_int),
+        "tg_domain_destroy": ([P], ctypes.c_int),
+        "tg_tractogram": ([AP, P, P, P, U32, F, U32, P, P, P], ctypes.c_int),
+        "tg_tractogram_host": ([AP, P, P, P, U32, F, U32, P, P, P], ctypes.c_int),
+        "tg_tracker_create": ([U64, ctypes.POINTER(P)], ctypes.c_int),
+        "tg_tracker_destroy": ([P], ctypes.c_int),
+        "tg_tracker_run": ([P, AP, P, P, P, ctypes.c_int, U32, U32, P, F, U32, P, P,
+                            ctypes.POINTER(U64), ctypes.POINTER(U64), P], ctypes.c_int),
+        "tg_tracker_stats": ([P, ctypes.POINTER(F), ctypes.POINTER(U32), ctypes.POINTER(U32)], ctypes.c_int),
+        "tg_tracker_copy_points": ([P, P, U64, U64, ctypes.c_int, P], ctypes.c_int),
+        "tg_seeds_from_fod": ([I32, U32, P, P, U32, P, P, U32, P, P], ctypes.c_int),
+        "tg_domain_contains": ([P, P, U32, P, P], ctypes.c_int),
+        "tg_field_evaluate": ([P, P, U32, P, P], ctypes.c_int),
+        "tg_local_evaluate": ([I32, U32, P, P, U32, P, P], ctypes.c_int),
+        "tg_update_orientation": ([I32, U32, AP, P, P, U32, P, P], ctypes.c_int),
+        "tg_rng_stream": ([I32, U32, U32, U32, U32, P, P], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    """Raise the matching Python exception for a non-zero status."""
+    if status == TG_OK:
+        return
+    message = load().tg_last_error().decode(errors="replace")
+    if status == TG_ERR_INVALID_ARGUMENT:
+        raise ValueError(message)
+    if status == TG_ERR_UNSUPPORTED:
+        raise NotImplementedError(message)
+    if status == TG_ERR_OUT_OF_MEMORY:
+        raise MemoryError(message)
+    raise TgError(status, message)

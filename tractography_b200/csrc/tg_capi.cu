@@ -1,0 +1,647 @@
+/*
+ * tg_capi.cu -- the C ABI declared in include/tractography_b200.h.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tg_internal.h"
+#include "tractography_b200.h"
+
+using namespace tg;
+
+struct tg_field {
+    FieldDev d;
+};
+
+struct tg_domain {
+    DomainDev d;
+};
+
+struct tg_tracker {
+    uint64_t pool_points_request = 0;
+    // chunk pool
+    float* pool = nullptr;
+    int32_t* chunk_next = nullptr;
+    uint32_t n_chunks = 0;
+    // counters: [0] items, [1] steps; chunk counter separately
+    unsigned long long* counters = nullptr;
+    unsigned int* chunk_counter = nullptr;
+    // per-seed buffers
+    int32_t* first_chunk = nullptr;
+    uint32_t* lengths = nullptr;
+    uint64_t* offsets = nullptr;
+    uint32_t* ids = nullptr;
+    uint32_t* done_ids = nullptr;
+    size_t cap_seeds = 0;
+    float4* seeds = nullptr;
+    size_t cap_seed_copy = 0;
+    uint32_t* batch_seeds = nullptr;
+    size_t cap_batches = 0;
+    // packed output
+    float* points = nullptr;
+    uint64_t cap_points = 0;
+    uint64_t total_points = 0;
+    // host staging
+    std::vector<uint32_t> h_len;
+    std::vector<uint32_t> h_done;
+    std::vector<uint32_t> h_retry;
+    // statistics of the last run
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    float kernel_ms = 0.0f;
+    uint32_t waves = 0;
+    uint32_t launches = 0;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg)
+{
+    g_error = msg;
+    return code;
+}
+
+int fail_cuda(cudaError_t e, const char* what)
+{
+    const int code = (e == cudaErrorMemoryAllocation) ? TG_ERR_OUT_OF_MEMORY : TG_ERR_CUDA;
+    return fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define TG_TRY(call)                                     \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return fail_cuda(e_, #call); \
+    } while (0)
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+Grid grid_of(const float* inv, uint32_t nx, uint32_t ny, uint32_t nz)
+{
+    Grid g;
+    g.row0 = make_float4(inv[0], inv[1], inv[2], inv[3]);
+    g.row1 = make_float4(inv[4], inv[5], inv[6], inv[7]);
+    g.row2 = make_float4(inv[8], inv[9], inv[10], inv[11]);
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    return g;
+}
+
+int check_algorithm(const tg_algorithm* a)
+{
+    if (a == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "algorithm is null");
+    if (a->algorithm != TG_ALGO_TRANSPORT && a->algorithm != TG_ALGO_DIFFUSION)
+        return fail(TG_ERR_UNSUPPORTED, "unsupported algorithm id");
+    if (!std::isfinite(a->step_size) || a->step_size <= 0.0f)
+        return fail(TG_ERR_INVALID_ARGUMENT, "step_size must be finite and positive");
+    if (!std::isfinite(a->gamma)) return fail(TG_ERR_INVALID_ARGUMENT, "gamma must be finite");
+    if (a->algorithm == TG_ALGO_DIFFUSION && (!std::isfinite(a->noise_variance) || a->noise_variance < 0.0f))
+        return fail(TG_ERR_INVALID_ARGUMENT, "noise_variance must be finite and non-negative");
+    if (a->rng_mode != TG_RNG_MWC64X && a->rng_mode != TG_RNG_PHILOX)
+        return fail(TG_ERR_UNSUPPORTED, "unsupported rng_mode");
+    return TG_OK;
+}
+
+AlgoParams algo_params(const tg_algorithm* a)
+{
+    AlgoParams p;
+    p.step_size = a->step_size;
+    p.gamma = a->gamma;
+    p.noise_variance = a->algorithm == TG_ALGO_DIFFUSION ? a->noise_variance : 0.0f;
+    // algorithm.py:106 and 222-225, evaluated in binary32 as the kernel would.
+    p.scale_drift = a->gamma * a->step_size;
+    p.scale_noise = sqrtf(p.noise_variance * a->gamma * a->step_size);
+    p.rng_mode = a->rng_mode;
+    p.philox_key = a->philox_key;
+    return p;
+}
+
+int make_track_params(const tg_algorithm* a, const tg_domain* d, const tg_field* f, float save_at,
+                      uint32_t n_steps, TrackParams* out)
+{
+    int st = check_algorithm(a);
+    if (st != TG_OK) return st;
+    if (d == nullptr || f == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "domain and field are required");
+    if (!std::isfinite(save_at) || save_at <= 0.0f)
+        return fail(TG_ERR_INVALID_ARGUMENT, "save_at must be finite and positive");
+    TrackParams p;
+    std::memset(&p, 0, sizeof p);
+    p.dgrid = grid_of(d->d.inv_affine, d->d.nx, d->d.ny, d->d.nz);
+    p.mask = d->d.mask;
+    p.fgrid = grid_of(f->d.inv_affine, f->d.nx, f->d.ny, f->d.nz);
+    p.field = f->d.data;
+    p.cpad = f->d.cpad;
+    p.same_grid = d->d.nx == f->d.nx && d->d.ny == f->d.ny && d->d.nz == f->d.nz &&
+                  std::memcmp(d->d.inv_affine, f->d.inv_affine, 12 * sizeof(float)) == 0;
+    p.algorithm = a->algorithm;
+    p.algo = algo_params(a);
+    p.save_at = save_at;
+    p.n_steps = n_steps;
+    *out = p;
+    return TG_OK;
+}
+
+template <typename T>
+cudaError_t ensure(T** ptr, size_t* cap, size_t n)
+{
+    if (*cap >= n && *ptr != nullptr) return cudaSuccess;
+    if (*ptr) cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    const size_t want = std::max<size_t>(n, 1);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(ptr), want * sizeof(T));
+    if (e == cudaSuccess) *cap = want;
+    return e;
+}
+
+int sm_count()
+{
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tg_abi_version(void) { return TG_ABI_VERSION; }
+
+const char* tg_status_string(int status)
+{
+    switch (status) {
+    case TG_OK: return "ok";
+    case TG_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case TG_ERR_CUDA: return "CUDA error";
+    case TG_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case TG_ERR_UNSUPPORTED: return "unsupported";
+    case TG_ERR_POOL_EXHAUSTED: return "point pool exhausted";
+    default: return "unknown status";
+    }
+}
+
+const char* tg_last_error(void) { return g_error.c_str(); }
+
+int tg_field_create(int32_t model, const float* values, uint32_t nx, uint32_t ny, uint32_t nz,
+                    uint32_t n_parameters, const float inverse_affine[16], void* stream, tg_field** out)
+{
+    if (out == nullptr || values == nullptr || inverse_affine == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    if (nx == 0 || ny == 0 || nz == 0 || n_parameters == 0)
+        return fail(TG_ERR_INVALID_ARGUMENT, "field dimensions must be positive");
+    if (model == TG_MODEL_SH && n_parameters > 45)
+        return fail(TG_ERR_UNSUPPORTED, "spherical-harmonic fields support at most 45 coefficients (lmax 8)");
+    if (model == TG_MODEL_DTI && n_parameters != 6)
+        return fail(TG_ERR_INVALID_ARGUMENT, "tensor fields have 6 coefficients");
+    if (model != TG_MODEL_SH && model != TG_MODEL_DTI) return fail(TG_ERR_UNSUPPORTED, "unknown model");
+    tg_field* f = new tg_field();
+    f->d.nx = nx;
+    f->d.ny = ny;
+    f->d.nz = nz;
+    f->d.n_params = n_parameters;
+    f->d.model = model;
+    f->d.lmax = model == TG_MODEL_SH ? lmax_for(n_parameters) : 0;
+    f->d.cpad = model == TG_MODEL_SH ? (uint32_t)((n_coef_full(f->d.lmax) + 3) / 4 * 4) : 8u;
+    std::memcpy(f->d.inv_affine, inverse_affine, sizeof f->d.inv_affine);
+    const size_t nvox = (size_t)nx * ny * nz;
+    f->d.bytes = nvox * f->d.cpad * sizeof(float);
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&f->d.data), f->d.bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(f->d.data, 0, f->d.bytes, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(f->d.data, f->d.cpad * sizeof(float), values, n_parameters * sizeof(float),
+                              n_parameters * sizeof(float), nvox, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        if (f->d.data) cudaFree(f->d.data);
+        delete f;
+        return fail_cuda(e, "tg_field_create");
+    }
+    *out = f;
+    return TG_OK;
+}
+
+int tg_field_destroy(tg_field* field)
+{
+    if (field == nullptr) return TG_OK;
+    if (field->d.data) cudaFree(field->d.data);
+    delete field;
+    return TG_OK;
+}
+
+int tg_domain_create(const uint8_t* mask, uint32_t nx, uint32_t ny, uint32_t nz, const float inverse_affine[16],
+                     void* stream, tg_domain** out)
+{
+    if (out == nullptr || mask == nullptr || inverse_affine == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    if (nx == 0 || ny == 0 || nz == 0) return fail(TG_ERR_INVALID_ARGUMENT, "domain dimensions must be positive");
+    tg_domain* d = new tg_domain();
+    d->d.nx = nx;
+    d->d.ny = ny;
+    d->d.nz = nz;
+    std::memcpy(d->d.inv_affine, inverse_affine, sizeof d->d.inv_affine);
+    d->d.bytes = (size_t)nx * ny * nz;
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&d->d.mask), d->d.bytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d->d.mask, mask, d->d.bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        if (d->d.mask) cudaFree(d->d.mask);
+        delete d;
+        return fail_cuda(e, "tg_domain_create");
+    }
+    *out = d;
+    return TG_OK;
+}
+
+int tg_domain_destroy(tg_domain* domain)
+{
+    if (domain == nullptr) return TG_OK;
+    if (domain->d.mask) cudaFree(domain->d.mask);
+    delete domain;
+    return TG_OK;
+}
+
+int tg_tractogram(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field, const float* seeds,
+                  uint32_t n_seeds, float save_at, uint32_t n_steps, float* streamlines, uint32_t* lengths,
+                  void* stream)
+{
+    TrackParams p;
+    int st = make_track_params(algorithm, domain, field, save_at, n_steps, &p);
+    if (st != TG_OK) return st;
+    if (n_seeds == 0) return TG_OK;
+    if (n_steps == 0) return fail(TG_ERR_INVALID_ARGUMENT, "n_steps must be positive");
+    if (seeds == nullptr || streamlines == nullptr || lengths == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null buffer");
+    TG_TRY(launch_track_dense(field->d, p, reinterpret_cast<const float4*>(seeds), n_seeds, algorithm->rng_seed,
+                              algorithm->seed_offset, reinterpret_cast<float4*>(streamlines), lengths,
+                              as_stream(stream)));
+    return TG_OK;
+}
+
+int tg_tractogram_host(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
+                       const float* seeds, uint32_t n_seeds, float save_at, uint32_t n_steps, float* streamlines,
+                       uint32_t* lengths, void* stream)
+{
+    TrackParams p;
+    int st = make_track_params(algorithm, domain, field, save_at, n_steps, &p);
+    if (st != TG_OK) return st;
+    if (n_seeds == 0) return TG_OK;
+    if (n_steps == 0) return fail(TG_ERR_INVALID_ARGUMENT, "n_steps must be positive");
+    cudaStream_t s = as_stream(stream);
+    float* d_seeds = nullptr;
+    float* d_out = nullptr;
+    uint32_t* d_len = nullptr;
+    const size_t out_bytes = (size_t)n_seeds * n_steps * 4 * sizeof(float);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&d_seeds), (size_t)n_seeds * 8 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d_out), out_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d_len), (size_t)n_seeds * sizeof(uint32_t));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_seeds, seeds, (size_t)n_seeds * 8 * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = launch_track_dense(field->d, p, reinterpret_cast<const float4*>(d_seeds), n_seeds, algorithm->rng_seed,
+                               algorithm->seed_offset, reinterpret_cast<float4*>(d_out), d_len, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(streamlines, d_out, out_bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(lengths, d_len, (size_t)n_seeds * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_seeds);
+    cudaFree(d_out);
+    cudaFree(d_len);
+    if (e != cudaSuccess) return fail_cuda(e, "tg_tractogram_host");
+    return TG_OK;
+}
+
+int tg_tracker_create(uint64_t pool_points, tg_tracker** out)
+{
+    if (out == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    tg_tracker* t = new tg_tracker();
+    t->pool_points_request = pool_points;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&t->counters), 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&t->chunk_counter), sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaEventCreate(&t->ev_start);
+    if (e == cudaSuccess) e = cudaEventCreate(&t->ev_stop);
+    if (e != cudaSuccess) {
+        tg_tracker_destroy(t);
+        return fail_cuda(e, "tg_tracker_create");
+    }
+    *out = t;
+    return TG_OK;
+}
+
+int tg_tracker_destroy(tg_tracker* t)
+{
+    if (t == nullptr) return TG_OK;
+    cudaFree(t->pool);
+    cudaFree(t->chunk_next);
+    cudaFree(t->counters);
+    cudaFree(t->chunk_counter);
+    cudaFree(t->first_chunk);
+    cudaFree(t->lengths);
+    cudaFree(t->offsets);
+    cudaFree(t->ids);
+    cudaFree(t->done_ids);
+    cudaFree(t->seeds);
+    cudaFree(t->batch_seeds);
+    cudaFree(t->points);
+    if (t->ev_start) cudaEventDestroy(t->ev_start);
+    if (t->ev_stop) cudaEventDestroy(t->ev_stop);
+    delete t;
+    return TG_OK;
+}
+
+int tg_tracker_stats(const tg_tracker* t, float* kernel_ms, uint32_t* waves, uint32_t* launches)
+{
+    if (t == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "tracker is null");
+    if (kernel_ms) *kernel_ms = t->kernel_ms;
+    if (waves) *waves = t->waves;
+    if (launches) *launches = t->launches;
+    return TG_OK;
+}
+
+static int tracker_pool(tg_tracker* t, uint64_t want_points)
+{
+    uint64_t chunks = (want_points + kChunkPoints - 1) / kChunkPoints;
+    if (chunks < 1) chunks = 1;
+    if (chunks > 0x7fffffffull) chunks = 0x7fffffffull;
+    if (t->pool != nullptr && t->n_chunks >= chunks) return TG_OK;
+    cudaFree(t->pool);
+    cudaFree(t->chunk_next);
+    t->pool = nullptr;
+    t->chunk_next = nullptr;
+    t->n_chunks = 0;
+    TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->pool), (size_t)chunks * kChunkPoints * 3 * sizeof(float)));
+    TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->chunk_next), (size_t)chunks * sizeof(int32_t)));
+    t->n_chunks = (uint32_t)chunks;
+    return TG_OK;
+}
+
+static int tracker_points(tg_tracker* t, uint64_t need, cudaStream_t s)
+{
+    if (t->cap_points >= need && t->points != nullptr) return TG_OK;
+    uint64_t cap = std::max<uint64_t>(need, t->cap_points + t->cap_points / 2);
+    cap = std::max<uint64_t>(cap, 1);
+    float* np = nullptr;
+    TG_TRY(cudaMalloc(reinterpret_cast<void**>(&np), (size_t)cap * 3 * sizeof(float)));
+    if (t->points != nullptr && t->total_points > 0) {
+        cudaError_t e = cudaMemcpyAsync(np, t->points, (size_t)t->total_points * 3 * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            cudaFree(np);
+            return fail_cuda(e, "grow point buffer");
+        }
+    }
+    cudaFree(t->points);
+    t->points = np;
+    t->cap_points = cap;
+    return TG_OK;
+}
+
+int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
+                   const float* seeds, int seeds_on_host, uint32_t n_seeds, uint32_t batch_size,
+                   const uint32_t* batch_rng_seeds, float save_at, uint32_t n_steps, uint32_t* h_lengths,
+                   uint64_t* h_offsets, uint64_t* total_points, uint64_t* total_steps, void* stream)
+{
+    if (t == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "tracker is null");
+    TrackParams tp;
+    int st = make_track_params(algorithm, domain, field, save_at, n_steps, &tp);
+    if (st != TG_OK) return st;
+    t->total_points = 0;
+    t->kernel_ms = 0.0f;
+    t->waves = 0;
+    t->launches = 0;
+    if (total_points) *total_points = 0;
+    if (total_steps) *total_steps = 0;
+    if (n_seeds == 0) return TG_OK;
+    if (n_steps == 0) return fail(TG_ERR_INVALID_ARGUMENT, "n_steps must be positive");
+    if (batch_size == 0) return fail(TG_ERR_INVALID_ARGUMENT, "batch_size must be positive");
+    if (seeds == nullptr || batch_rng_seeds == nullptr || h_lengths == nullptr || h_offsets == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null buffer");
+    cudaStream_t s = as_stream(stream);
+    const uint32_t n_batches = (n_seeds + batch_size - 1) / batch_size;
+
+    TG_TRY(ensure(&t->batch_seeds, &t->cap_batches, n_batches));
+    TG_TRY(cudaMemcpyAsync(t->batch_seeds, batch_rng_seeds, n_batches * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    const float4* d_seeds = reinterpret_cast<const float4*>(seeds);
+    if (seeds_on_host) {
+        TG_TRY(ensure(&t->seeds, &t->cap_seed_copy, (size_t)n_seeds * 2));
+        TG_TRY(cudaMemcpyAsync(t->seeds, seeds, (size_t)n_seeds * 8 * sizeof(float), cudaMemcpyHostToDevice, s));
+        d_seeds = t->seeds;
+    }
+    if (t->cap_seeds < n_seeds) {
+        cudaFree(t->first_chunk);
+        cudaFree(t->lengths);
+        cudaFree(t->offsets);
+        cudaFree(t->ids);
+        cudaFree(t->done_ids);
+        t->first_chunk = nullptr;
+        t->lengths = nullptr;
+        t->offsets = nullptr;
+        t->ids = nullptr;
+        t->done_ids = nullptr;
+        t->cap_seeds = 0;
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->first_chunk), (size_t)n_seeds * sizeof(int32_t)));
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->lengths), (size_t)n_seeds * sizeof(uint32_t)));
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->offsets), (size_t)n_seeds * sizeof(uint64_t)));
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->ids), (size_t)n_seeds * sizeof(uint32_t)));
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->done_ids), (size_t)n_seeds * sizeof(uint32_t)));
+        t->cap_seeds = n_seeds;
+    }
+
+    // Pool: the worst case (every streamline fills n_steps points, rounded
+    // up to whole chunks) when it fits a third of free memory; otherwise
+    // the pool is smaller and streamlines that run out are re-tracked in a
+    // later wave (results depend only on the seed and its RNG stream).
+    const uint64_t per_seed = ((uint64_t)n_steps + kChunkPoints - 1) / kChunkPoints * kChunkPoints;
+    uint64_t want = t->pool_points_request;
+    if (want == 0) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const uint64_t budget = (uint64_t)(free_b / 3) / (3 * sizeof(float) + 1);
+        want = std::min<uint64_t>(per_seed * n_seeds, std::max<uint64_t>(budget, per_seed * 64));
+    }
+    st = tracker_pool(t, want);
+    if (st != TG_OK) return st;
+
+    PersistentParams pp;
+    std::memset(&pp, 0, sizeof pp);
+    pp.t = tp;
+    pp.seeds = d_seeds;
+    pp.n_seeds = n_seeds;
+    pp.batch_size = batch_size;
+    pp.batch_rng_seeds = t->batch_seeds;
+    pp.seed_offset = algorithm->seed_offset;
+    pp.item_counter = t->counters;
+    pp.steps_done = t->counters + 1;
+    pp.chunk_counter = t->chunk_counter;
+    pp.first_chunk = t->first_chunk;
+    pp.lengths = t->lengths;
+
+    const int block = persistent_block_size();
+    const int grid = sm_count() * persistent_blocks_per_sm(field->d, algorithm->algorithm);
+
+    t->h_len.resize(n_seeds);
+    TG_TRY(cudaMemsetAsync(t->counters + 1, 0, sizeof(unsigned long long), s));
+    uint64_t total = 0;
+    bool first_wave = true;
+    int stalls = 0;
+    std::vector<uint32_t> wave_items;
+    while (first_wave || !wave_items.empty()) {
+        const uint32_t n_items = first_wave ? n_seeds : (uint32_t)wave_items.size();
+        if (!first_wave)
+            TG_TRY(cudaMemcpyAsync(t->ids, wave_items.data(), n_items * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        pp.item_ids = first_wave ? nullptr : t->ids;
+        pp.n_items = n_items;
+        pp.pool = t->pool;
+        pp.chunk_next = t->chunk_next;
+        pp.n_chunks = t->n_chunks;
+        TG_TRY(cudaMemsetAsync(t->counters, 0, sizeof(unsigned long long), s));
+        TG_TRY(cudaMemsetAsync(t->chunk_counter, 0, sizeof(unsigned int), s));
+        TG_TRY(cudaEventRecord(t->ev_start, s));
+        TG_TRY(launch_track_persistent(field->d, pp, grid, block, s));
+        TG_TRY(cudaEventRecord(t->ev_stop, s));
+        TG_TRY(cudaMemcpyAsync(t->h_len.data(), t->lengths, (size_t)n_seeds * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost, s));
+        TG_TRY(cudaStreamSynchronize(s));
+        float wave_ms = 0.0f;
+        TG_TRY(cudaEventElapsedTime(&wave_ms, t->ev_start, t->ev_stop));
+        t->kernel_ms += wave_ms;
+        t->waves += 1;
+        t->launches += 1;
+
+        t->h_done.clear();
+        t->h_retry.clear();
+        for (uint32_t k = 0; k < n_items; ++k) {
+            const uint32_t i = first_wave ? k : wave_items[k];
+            const uint32_t L = t->h_len[i];
+            if (L & kOverflowBit) {
+                t->h_retry.push_back(i);
+            } else {
+                t->h_done.push_back(i);
+                h_offsets[i] = total;
+                h_lengths[i] = L;
+                total += L;
+            }
+        }
+        if (t->h_done.empty()) {
+            // No streamline fit: grow the pool and repeat the wave.
+            if (++stalls > 4) return fail(TG_ERR_POOL_EXHAUSTED, "point pool too small for one streamline");
+            st = tracker_pool(t, (uint64_t)t->n_chunks * kChunkPoints * 4);
+            if (st != TG_OK) return st;
+            wave_items.assign(t->h_retry.begin(), t->h_retry.end());
+            first_wave = false;
+            continue;
+        }
+        st = tracker_points(t, total, s);
+        if (st != TG_OK) return st;
+        TG_TRY(cudaMemcpyAsync(t->offsets, h_offsets, (size_t)n_seeds * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+        TG_TRY(cudaMemcpyAsync(t->done_ids, t->h_done.data(), t->h_done.size() * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, s));
+        TG_TRY(launch_gather(t->pool, t->chunk_next, t->first_chunk, t->lengths, t->offsets, t->done_ids,
+                             (uint32_t)t->h_done.size(), t->points, s));
+        t->launches += 1;
+        t->total_points = total;
+        wave_items.assign(t->h_retry.begin(), t->h_retry.end());
+        first_wave = false;
+    }
+    unsigned long long steps = 0;
+    TG_TRY(cudaMemcpyAsync(&steps, t->counters + 1, sizeof steps, cudaMemcpyDeviceToHost, s));
+    TG_TRY(cudaStreamSynchronize(s));
+    t->total_points = total;
+    if (total_points) *total_points = total;
+    if (total_steps) *total_steps = steps;
+    return TG_OK;
+}
+
+int tg_tracker_copy_points(tg_tracker* t, float* dst, uint64_t first, uint64_t count, int dst_on_host, void* stream)
+{
+    if (t == nullptr || (dst == nullptr && count > 0)) return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    if (first + count > t->total_points) return fail(TG_ERR_INVALID_ARGUMENT, "point range out of bounds");
+    if (count == 0) return TG_OK;
+    cudaStream_t s = as_stream(stream);
+    TG_TRY(cudaMemcpyAsync(dst, t->points + first * 3, (size_t)count * 3 * sizeof(float),
+                           dst_on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    if (dst_on_host) TG_TRY(cudaStreamSynchronize(s));
+    return TG_OK;
+}
+
+int tg_seeds_from_fod(int32_t model, uint32_t n_coefficients, const float* fod, const float* voxels, uint32_t nnz,
+                      const float* affine, const uint32_t* states, uint32_t n_seeds, float* seeds, void* stream)
+{
+    if (n_seeds == 0) return TG_OK;
+    if (fod == nullptr || voxels == nullptr || affine == nullptr || states == nullptr || seeds == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null buffer");
+    if (nnz == 0) return fail(TG_ERR_INVALID_ARGUMENT, "the FOD has no nonzero voxel");
+    if (model == TG_MODEL_SH && (n_coefficients == 0 || n_coefficients > 45))
+        return fail(TG_ERR_UNSUPPORTED, "spherical-harmonic FODs support 1..45 coefficients");
+    if (model == TG_MODEL_DTI && n_coefficients != 6) return fail(TG_ERR_INVALID_ARGUMENT, "tensors have 6 coefficients");
+    TG_TRY(launch_seeds_from_fod(model, n_coefficients, fod, reinterpret_cast<const float4*>(voxels), nnz, affine,
+                                 reinterpret_cast<const uint2*>(states), n_seeds, reinterpret_cast<float4*>(seeds),
+                                 as_stream(stream)));
+    return TG_OK;
+}
+
+int tg_domain_contains(const tg_domain* domain, const float* points, uint32_t n, uint8_t* out, void* stream)
+{
+    if (domain == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "domain is null");
+    if (n == 0) return TG_OK;
+    TG_TRY(launch_contains(domain->d, reinterpret_cast<const float4*>(points), n, out, as_stream(stream)));
+    return TG_OK;
+}
+
+int tg_field_evaluate(const tg_field* field, const float* points, uint32_t n, float* out, void* stream)
+{
+    if (field == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "field is null");
+    if (n == 0) return TG_OK;
+    TG_TRY(launch_field_evaluate(field->d, reinterpret_cast<const float4*>(points), n, out, as_stream(stream)));
+    return TG_OK;
+}
+
+int tg_local_evaluate(int32_t model, uint32_t n_parameters, const float* parameters, const float* orientations,
+                      uint32_t n, float* out, void* stream)
+{
+    if (model == TG_MODEL_SH && (n_parameters == 0 || n_parameters > 45))
+        return fail(TG_ERR_UNSUPPORTED, "spherical-harmonic models support 1..45 coefficients");
+    if (model == TG_MODEL_DTI && n_parameters != 6) return fail(TG_ERR_INVALID_ARGUMENT, "tensors have 6 coefficients");
+    if (model != TG_MODEL_SH && model != TG_MODEL_DTI) return fail(TG_ERR_UNSUPPORTED, "unknown model");
+    if (n == 0) return TG_OK;
+    TG_TRY(launch_local_evaluate(model, n_parameters, parameters, reinterpret_cast<const float4*>(orientations), n,
+                                 out, as_stream(stream)));
+    return TG_OK;
+}
+
+int tg_update_orientation(int32_t model, uint32_t n_parameters, const tg_algorithm* algorithm,
+                          const float* parameters, const float* orientations, uint32_t n, float* out, void* stream)
+{
+    int st = check_algorithm(algorithm);
+    if (st != TG_OK) return st;
+    if (model == TG_MODEL_SH && (n_parameters == 0 || n_parameters > 45))
+        return fail(TG_ERR_UNSUPPORTED, "spherical-harmonic models support 1..45 coefficients");
+    if (model == TG_MODEL_DTI && n_parameters != 6) return fail(TG_ERR_INVALID_ARGUMENT, "tensors have 6 coefficients");
+    if (model != TG_MODEL_SH && model != TG_MODEL_DTI) return fail(TG_ERR_UNSUPPORTED, "unknown model");
+    if (n == 0) return TG_OK;
+    TG_TRY(launch_update_orientation(model, n_parameters, algorithm->algorithm, algo_params(algorithm),
+                                     algorithm->rng_seed, algorithm->seed_offset, parameters,
+                                     reinterpret_cast<const float4*>(orientations), n,
+                                     reinterpret_cast<float4*>(out), as_stream(stream)));
+    return TG_OK;
+}
+
+int tg_rng_stream(int32_t which, uint32_t s0, uint32_t s1, uint32_t n, uint32_t max, void* out, void* stream)
+{
+    if (which < 0 || which > 2) return fail(TG_ERR_INVALID_ARGUMENT, "which must be 0, 1 or 2");
+    if (n == 0) return TG_OK;
+    TG_TRY(launch_rng_streams(which, s0, s1, n, max, out, as_stream(stream)));
+    return TG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+/*
+ * tg_fmath.h -- portable, bit-reproducible binary32 transcendentals.
+ *
+ * Every function here is a fixed sequence of IEEE-754 binary32 operations
+ * (add, mul, fma, div, sqrt, rint, comparisons and exponent bit edits), so a
+ * CPU build (gcc, -ffp-contract=off, no fast-math) and a CUDA build
+ * (nvcc -fmad=false, IEEE div/sqrt, no flush-to-zero) return the same bits
+ * for the same input.  The streamline integrator is sensitive to the last
+ * bit (the Transport orientation update at a 0.1-voxel step amplifies a
+ * 1e-7 perturbation to whole voxels), so the tracking kernels and the CPU
+ * oracle share this layer the way OpenCL kernels share a platform libm.
+ *
+ * Methods (all coefficients derived from the mathematics, not from any
+ * vendor library):
+ *   - argument reduction: Cody & Waite (1980) with the constant split into
+ *     three binary32 parts and fused multiply-adds;
+ *   - sin/cos on |r| <= pi/4: truncated Taylor series (terms to r^9 / r^10,
+ *     truncation error < 0.05 ulp), Horner form;
+ *   - exp on |r| <= ln2/2: Taylor series to r^7, scaled by 2^k in two exact
+ *     steps;
+ *   - log: x = m * 2^e with m in [sqrt(1/2), sqrt(2)), log(m) = 2 atanh(s),
+ *     s = (m-1)/(m+1), odd series to s^9.
+ * Measured accuracy against double-precision libm is checked by the tests
+ * (max error <= 2 ulp over dense sweeps).
+ */
+#ifndef TG_FMATH_H
+#define TG_FMATH_H
+
+#include <stdint.h>
+#ifndef __CUDACC__
+#include <math.h>
+#include <string.h>
+#endif
+
+#if defined(__CUDACC__)
+#define TGM_FN __host__ __device__ __forceinline__
+#else
+#define TGM_FN static inline
+#endif
+
+/* Constants (hexadecimal binary32 values). */
+#define TGM_PI        0x1.921fb6p+1f     /* float(pi) */
+#define TGM_TWO_PI    0x1.921fb6p+2f     /* 2 * float(pi), exact */
+#define TGM_2_OVER_PI 0x1.45f306p-1f
+#define TGM_PIO2_A    0x1.921fb6p+0f     /* pi/2 = A + B + C */
+#define TGM_PIO2_B   -0x1.777a5cp-25f
+#define TGM_PIO2_C   -0x1.ee59dap-50f
+#define TGM_LOG2E     0x1.715476p+0f
+#define TGM_LN2_HI    0x1.62e430p-1f     /* ln2 = HI + LO */
+#define TGM_LN2_LO   -0x1.05c610p-29f
+#define TGM_SQRT2     0x1.6a09e6p+0f
+
+TGM_FN uint32_t tgm_f2u(float x)
+{
+#if defined(__CUDA_ARCH__)
+    return __float_as_uint(x);
+#else
+    uint32_t u;
+    memcpy(&u, &x, sizeof u);
+    return u;
+#endif
+}
+
+TGM_FN float tgm_u2f(uint32_t u)
+{
+#if defined(__CUDA_ARCH__)
+    return __uint_as_float(u);
+#else
+    float x;
+    memcpy(&x, &u, sizeof x);
+    return x;
+#endif
+}
+
+/* 2^k as a binary32 value for k in [-126, 127]. */
+TGM_FN float tgm_pow2i(int k)
+{
+    return tgm_u2f((uint32_t)(k + 127) << 23);
+}
+
+/* Quadrant index from the rounded reduction multiple (NaN/huge -> 0). */
+TGM_FN int tgm_quadrant(float q)
+{
+    return (q == q && fabsf(q) < 8388608.0f) ? (int)q : 0;
+}
+
+/*
+ * sincos: s = sin(x), c = cos(x).  Reduction x = q*pi/2 + r, |r| <~ pi/4.
+ */
+TGM_FN void tgm_sincosf(float x, float* s_out, float* c_out)
+{
+    const float q = rintf(x * TGM_2_OVER_PI);
+    float r = fmaf(-q, TGM_PIO2_A, x);
+    r = fmaf(-q, TGM_PIO2_B, r);
+    r = fmaf(-q, TGM_PIO2_C, r);
+    const float r2 = r * r;
+
+    /* sin r = r + r^3 (-1/3! + r^2 (1/5! + r^2 (-1/7! + r^2 / 9!))) */
+    float ps = 0x1.71de3ap-19f;                  /*  1/9! */
+    ps = fmaf(ps, r2, -0x1.a01a02p-13f);         /* -1/7! */
+    ps = fmaf(ps, r2, 0x1.111112p-7f);           /*  1/5! */
+    ps = fmaf(ps, r2, -0x1.555556p-3f);          /* -1/3! */
+    const float sr = fmaf(r * r2, ps, r);
+
+    /* cos r = 1 + r^2 (-1/2 + r^2 (1/4! + r^2 (-1/6! + r^2 (1/8! - r^2/10!)))) */
+    float pc = -0x1.27e4fcp-22f;                 /* -1/10! */
+    pc = fmaf(pc, r2, 0x1.a01a02p-16f);          /*  1/8!  */
+    pc = fmaf(pc, r2, -0x1.6c16c2p-10f);         /* -1/6!  */
+    pc = fmaf(pc, r2, 0x1.555556p-5f);           /*  1/4!  */
+    pc = fmaf(pc, r2, -0.5f);
+    const float cr = fmaf(r2, pc, 1.0f);
+
+    const int quadrant = tgm_quadrant(q) & 3;
+    float s, c;
+    if (quadrant == 0) { s = sr;  c = cr;  }
+    else if (quadrant == 1) { s = cr;  c = -sr; }
+    else if (quadrant == 2) { s = -sr; c = -cr; }
+    else { s = -cr; c = sr;  }
+    *s_out = s;
+    *c_out = c;
+}
+
+TGM_FN float tgm_cosf(float x)
+{
+    float s, c;
+    tgm_sincosf(x, &s, &c);
+    return c;
+}
+
+TGM_FN float tgm_sinf(float x)
+{
+    float s, c;
+    tgm_sincosf(x, &s, &c);
+    return s;
+}
+
+/*
+ * exp: x = k ln2 + r, |r| <= ln2/2; e^r by Taylor to r^7; scale by 2^k.
+ */
+TGM_FN float tgm_expf(float x)
+{
+    if (x != x) return x;
+    if (x > 88.72284f) return tgm_u2f(0x7f800000u);   /* +inf */
+    if (x < -103.97208f) return 0.0f;
+    const float k = rintf(x * TGM_LOG2E);
+    float r = fmaf(-k, TGM_LN2_HI, x);
+    r = fmaf(-k, TGM_LN2_LO, r);
+    float p = 0x1.a01a02p-13f;                   /* 1/7! */
+    p = fmaf(p, r, 0x1.6c16c2p-10f);             /* 1/6! */
+    p = fmaf(p, r, 0x1.111112p-7f);              /* 1/5! */
+    p = fmaf(p, r, 0x1.555556p-5f);              /* 1/4! */
+    p = fmaf(p, r, 0x1.555556p-3f);              /* 1/3! */
+    p = fmaf(p, r, 0.5f);
+    p = fmaf(p, r, 1.0f);
+    p = fmaf(p, r, 1.0f);
+    const int ki = (int)k;                       /* |k| <= 150 here */
+    const int k1 = ki / 2;
+    const int k2 = ki - k1;
+    return (p * tgm_pow2i(k1)) * tgm_pow2i(k2);
+}
+
+/*
+ * log: natural logarithm for binary32.
+ */
+TGM_FN float tgm_logf(float x)
+{
+    if (x != x) return x;
+    if (x < 0.0f) return tgm_u2f(0x7fc00000u);        /* NaN */
+    if (x == 0.0f) return tgm_u2f(0xff800000u);       /* -inf */
+    if (x == tgm_u2f(0x7f800000u)) return x;          /* +inf */
+    int e_adjust = 0;
+    if (x < 0x1p-126f) {                              /* subnormal input */
+        x = x * 0x1p+24f;
+        e_adjust = -24;
+    }
+    const uint32_t bits = tgm_f2u(x);
+    int e = (int)((bits >> 23) & 0xffu) - 127 + e_adjust;
+    float m = tgm_u2f((bits & 0x007fffffu) | 0x3f800000u);   /* [1, 2) */
+    if (m > TGM_SQRT2) {
+        m = m * 0.5f;
+        e = e + 1;
+    }
+    const float f = m - 1.0f;                         /* exact */
+    const float s = f / (2.0f + f);
+    const float z = s * s;
+    /* log(m) = 2s (1 + z/3 + z^2/5 + z^3/7 + z^4/9) */
+    float p = 0x1.c71c72p-4f;                         /* 1/9 */
+    p = fmaf(p, z, 0x1.24924ap-3f);                   /* 1/7 */
+    p = fmaf(p, z, 0x1.99999ap-3f);                   /* 1/5 */
+    p = fmaf(p, z, 0x1.555556p-2f);                   /* 1/3 */
+    const float two_s = s + s;
+    const float logm = fmaf(two_s * z, p, two_s);
+    const float ef = (float)e;
+    return fmaf(ef, TGM_LN2_HI, fmaf(ef, TGM_LN2_LO, logm));
+}
+
+#endif /* TG_FMATH_H */

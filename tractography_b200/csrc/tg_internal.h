@@ -1,0 +1,115 @@
+/*
+ * tg_internal.h -- structures shared by the CUDA launchers and the C-ABI.
+ */
+#ifndef TG_INTERNAL_H
+#define TG_INTERNAL_H
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "tg_device.cuh"
+
+namespace tg {
+
+constexpr int kChunkPoints = 32;   // points per output chunk (chunk = 32 x 12 B)
+
+// Device-resident image field (field.py:52-122): float32 coefficients,
+// voxel-major (x, y, z) C order, each voxel padded to cpad floats
+// (cpad = round_up(full band, 4)) so a voxel loads as float4s.
+struct FieldDev {
+    float* data = nullptr;
+    uint32_t nx = 0, ny = 0, nz = 0;
+    uint32_t n_params = 0;     // C as given by the caller
+    uint32_t cpad = 0;
+    int model = kModelSH;      // SH unless created as a tensor field
+    int lmax = 0;
+    float inv_affine[16];
+    size_t bytes = 0;
+};
+
+// Device-resident image domain (domain.py:267-398): uint8 mask, same voxel
+// order as the reference's int32 mask.
+struct DomainDev {
+    uint8_t* mask = nullptr;
+    uint32_t nx = 0, ny = 0, nz = 0;
+    float inv_affine[16];
+    size_t bytes = 0;
+};
+
+// Everything one tracking launch needs, by value.
+struct TrackParams {
+    Grid dgrid;
+    const uint8_t* mask;
+    Grid fgrid;
+    const float* field;
+    uint32_t cpad;
+    int same_grid;           // domain and field inverse affines/dims identical
+    int algorithm;           // kTransport or kDiffusion
+    AlgoParams algo;
+    float save_at;
+    uint32_t n_steps;
+};
+
+// Batched persistent launch over work items 0..n_items-1; item k tracks
+// seed item_ids[k] (or k when item_ids is null).  Seed i belongs to batch
+// i / batch_size with stream id i % batch_size (tracking.py:105,115,
+// __init__.py:525), which keeps the reference's per-batch MWC64X streams.
+constexpr uint32_t kOverflowBit = 0x80000000u;   // in lengths[]: pool ran out
+
+struct PersistentParams {
+    TrackParams t;
+    const float4* seeds;          // (n_seeds, 2) float4
+    uint32_t n_seeds;
+    const uint32_t* item_ids;     // nullable
+    uint32_t n_items;
+    uint32_t batch_size;
+    const uint32_t* batch_rng_seeds;
+    uint64_t seed_offset;         // Philox index base
+    unsigned long long* item_counter;
+    // output: chunk pool
+    float* pool;                  // n_chunks * kChunkPoints * 3 floats
+    int32_t* chunk_next;          // n_chunks
+    uint32_t n_chunks;
+    unsigned int* chunk_counter;
+    int32_t* first_chunk;         // n_seeds
+    uint32_t* lengths;            // n_seeds; kOverflowBit set when retried
+    unsigned long long* steps_done;   // total accepted steps
+};
+
+// Launchers (tg_track.cu).
+cudaError_t launch_track_dense(const FieldDev& f, const TrackParams& p, const float4* seeds,
+                               uint32_t n_seeds, uint32_t rng_seed, uint64_t seed_offset,
+                               float4* out, uint32_t* lengths, cudaStream_t stream);
+cudaError_t launch_track_persistent(const FieldDev& f, const PersistentParams& p, int grid,
+                                    int block, cudaStream_t stream);
+cudaError_t launch_gather(const float* pool, const int32_t* chunk_next, const int32_t* first_chunk,
+                          const uint32_t* lengths, const uint64_t* offsets, const uint32_t* seed_ids,
+                          uint32_t n_ids, float* out_points, cudaStream_t stream);
+
+// Unit hooks (tg_aux.cu).
+cudaError_t launch_contains(const DomainDev& d, const float4* points, uint32_t n, uint8_t* out,
+                            cudaStream_t stream);
+cudaError_t launch_field_evaluate(const FieldDev& f, const float4* points, uint32_t n, float* out,
+                                  cudaStream_t stream);
+cudaError_t launch_local_evaluate(int model, uint32_t n_params, const float* params,
+                                  const float4* orientations, uint32_t n, float* out,
+                                  cudaStream_t stream);
+cudaError_t launch_update_orientation(int model, uint32_t n_params, int algorithm,
+                                      const AlgoParams& a, uint32_t rng_seed, uint64_t seed_offset,
+                                      const float* params, const float4* orientations, uint32_t n,
+                                      float4* out, cudaStream_t stream);
+cudaError_t launch_seeds_from_fod(int model, uint32_t n_coefficients, const float* fod,
+                                  const float4* voxels, uint32_t nnz, const float* affine,
+                                  const uint2* states, uint32_t n_seeds, float4* seeds,
+                                  cudaStream_t stream);
+cudaError_t launch_rng_streams(int which, uint32_t s0, uint32_t s1, uint32_t n, uint32_t max,
+                               void* out, cudaStream_t stream);
+
+int lmax_for(uint32_t n_params);
+int persistent_block_size();
+int persistent_blocks_per_sm(const FieldDev& f, int algorithm);
+
+}  // namespace tg
+
+#endif

@@ -1,0 +1,379 @@
+/*
+ * tg_track.cu -- streamline tracking kernels for sm_100a.
+ *
+ * Two forms of the reference's `tractogram` kernel (tracking.py:93-149):
+ *
+ *   track_dense_kernel       one thread per seed, dense (n, n_steps, float4)
+ *                            output exactly as the reference lays it out.
+ *                            This is the plain one-launch-per-batch form.
+ *
+ *   track_persistent_kernel  a grid sized to the GPU (blocks-per-SM x 148)
+ *                            whose lanes pull seeds from a device counter and
+ *                            refill as soon as their streamline terminates,
+ *                            so a warp never idles behind its longest
+ *                            streamline.  Points go to a pool of 32-point
+ *                            chunks linked per streamline; gather_kernel
+ *                            packs them into one (total_points, 3) array.
+ *                            Memory scales with the points produced, not with
+ *                            n_seeds x n_steps.
+ *
+ * Both run the identical per-step arithmetic of tg_device.cuh.  Field
+ * coefficients of the current voxel stay in registers and are reloaded only
+ * when the nearest voxel changes (every ~10 steps at a 0.1-voxel step,
+ * every ~1250 steps at 0.001 mm in 1.25 mm voxels).
+ */
+#include <cuda_runtime.h>
+
+#include "tg_internal.h"
+
+namespace tg {
+
+template <int MODEL, int LMAX>
+struct ModelShape {
+    static constexpr int CP = (MODEL == kModelDTI) ? 6 : n_coef_full(LMAX);
+    static constexpr int CPAD = (CP + 3) / 4 * 4;
+};
+
+struct Lane {
+    float px, py, pz;
+    float ox, oy, oz;
+    float time;
+    uint32_t n;
+    RngState rng;
+    int64_t cached;
+    uint32_t steps;
+};
+
+// One iteration of tracking.py:121-147 after the n < N_STEPS test.
+// Returns 0 when the streamline stops (domain or field check failed),
+// 1 after a step without a saved point, 2 after a step that saved point q.
+template <int MODEL, int LMAX, int ALGO, int CPAD>
+__device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (&c)[CPAD],
+                                          float& qx, float& qy, float& qz)
+{
+    // domain.py:358-382 and field.py:88-114 share the voxel-space point when
+    // both images have the same grid (the default of tg.tractogram).
+    const float ax = dot4(p.dgrid.row0, s.px, s.py, s.pz, 1.0f);
+    const float ay = dot4(p.dgrid.row1, s.px, s.py, s.pz, 1.0f);
+    const float az = dot4(p.dgrid.row2, s.px, s.py, s.pz, 1.0f);
+    {
+        const float vx = floorf(ax + 0.5f), vy = floorf(ay + 0.5f), vz = floorf(az + 0.5f);
+        if (!(vx >= 0.0f && vx < (float)p.dgrid.nx && vy >= 0.0f && vy < (float)p.dgrid.ny &&
+              vz >= 0.0f && vz < (float)p.dgrid.nz))
+            return 0;
+        const int64_t k = ((int64_t)(int32_t)vx * p.dgrid.ny + (int32_t)vy) * p.dgrid.nz + (int32_t)vz;
+        if (__ldg(p.mask + k) == 0) return 0;
+    }
+    float bx = ax, by = ay, bz = az;
+    if (!p.same_grid) {
+        bx = dot4(p.fgrid.row0, s.px, s.py, s.pz, 1.0f);
+        by = dot4(p.fgrid.row1, s.px, s.py, s.pz, 1.0f);
+        bz = dot4(p.fgrid.row2, s.px, s.py, s.pz, 1.0f);
+    }
+    const float fx = rintf(bx), fy = rintf(by), fz = rintf(bz);
+    if (!(fx >= 0.0f && fx < (float)p.fgrid.nx && fy >= 0.0f && fy < (float)p.fgrid.ny &&
+          fz >= 0.0f && fz < (float)p.fgrid.nz))
+        return 0;
+    const int64_t fv = ((int64_t)(int32_t)fx * p.fgrid.ny + (int32_t)fy) * p.fgrid.nz + (int32_t)fz;
+    if (fv != s.cached) {
+        const float4* src = reinterpret_cast<const float4*>(p.field) + fv * (CPAD / 4);
+#pragma unroll
+        for (int k = 0; k < CPAD / 4; ++k) {
+            const float4 v = __ldg(src + k);
+            c[4 * k] = v.x;
+            c[4 * k + 1] = v.y;
+            c[4 * k + 2] = v.z;
+            c[4 * k + 3] = v.w;
+        }
+        s.cached = fv;
+    }
+
+    update_orientation<MODEL, LMAX, ALGO>(p.algo, c, s.ox, s.oy, s.oz, s.rng);
+    s.steps += 1u;
+
+    const float step = p.algo.step_size;
+    s.px = fmaf(step, s.ox, s.px);
+    s.py = fmaf(step, s.oy, s.py);
+    s.pz = fmaf(step, s.oz, s.pz);
+    s.time = s.time + step;
+    if (s.time >= p.save_at) {
+        s.time = s.time - p.save_at;
+        qx = fmaf(-s.time, s.ox, s.px);
+        qy = fmaf(-s.time, s.oy, s.py);
+        qz = fmaf(-s.time, s.oz, s.pz);
+        return 2;
+    }
+    return 1;
+}
+
+__device__ __forceinline__ void lane_init(Lane& s, float4 a, float4 b, uint32_t rng_seed,
+                                          uint32_t stream_id, uint64_t index)
+{
+    s.px = a.x; s.py = a.y; s.pz = a.z;
+    s.ox = b.x; s.oy = b.y; s.oz = b.z;
+    s.time = 0.0f;
+    s.n = 1;
+    s.rng.mwc = rng_init(rng_seed, stream_id);
+    s.rng.index = index;
+    s.rng.step = 0u;
+    s.cached = -1;
+    s.steps = 0u;
+}
+
+// ------------------------------------------------------------------ dense
+
+template <int MODEL, int LMAX, int ALGO>
+__global__ void __launch_bounds__(128) track_dense_kernel(TrackParams p, const float4* __restrict__ seeds,
+                                                          uint32_t n_seeds, uint32_t rng_seed,
+                                                          uint64_t seed_offset, float4* __restrict__ out,
+                                                          uint32_t* __restrict__ lengths)
+{
+    constexpr int CPAD = ModelShape<MODEL, LMAX>::CPAD;
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= n_seeds) return;
+    Lane s;
+    const float4 a = seeds[2 * (size_t)gid];
+    const float4 b = seeds[2 * (size_t)gid + 1];
+    lane_init(s, a, b, rng_seed, gid, seed_offset + gid);
+    float c[CPAD];
+#pragma unroll
+    for (int k = 0; k < CPAD; ++k) c[k] = 0.0f;
+    float4* line = out + (size_t)gid * p.n_steps;
+    line[0] = a;
+    while (s.n < p.n_steps) {
+        float qx, qy, qz;
+        const int r = track_step<MODEL, LMAX, ALGO, CPAD>(p, s, c, qx, qy, qz);
+        if (r == 0) break;
+        if (r == 2) {
+            line[s.n] = make_float4(qx, qy, qz, 1.0f);
+            s.n++;
+        }
+    }
+    lengths[gid] = s.n;
+}
+
+// ------------------------------------------------------------- persistent
+
+__device__ __forceinline__ bool chunk_alloc(const PersistentParams& pp, int32_t& chunk)
+{
+    const unsigned int nc = atomicAdd(pp.chunk_counter, 1u);
+    if (nc >= pp.n_chunks) return false;
+    pp.chunk_next[nc] = -1;
+    chunk = (int32_t)nc;
+    return true;
+}
+
+__device__ __forceinline__ bool emit_point(const PersistentParams& pp, int32_t& chunk, uint32_t& fill,
+                                           float x, float y, float z)
+{
+    if (fill == (uint32_t)kChunkPoints) {
+        int32_t nc;
+        if (!chunk_alloc(pp, nc)) return false;
+        pp.chunk_next[chunk] = nc;
+        chunk = nc;
+        fill = 0;
+    }
+    float* q = pp.pool + ((size_t)chunk * kChunkPoints + fill) * 3;
+    q[0] = x;
+    q[1] = y;
+    q[2] = z;
+    fill++;
+    return true;
+}
+
+template <int MODEL, int LMAX, int ALGO>
+__global__ void __launch_bounds__(128) track_persistent_kernel(const PersistentParams pp)
+{
+    constexpr int CPAD = ModelShape<MODEL, LMAX>::CPAD;
+    const TrackParams& p = pp.t;
+    float c[CPAD];
+#pragma unroll
+    for (int k = 0; k < CPAD; ++k) c[k] = 0.0f;
+
+    Lane s;
+    int32_t chunk = -1;
+    uint32_t fill = 0;
+    uint32_t item = 0;
+    bool live = false;
+    unsigned long long steps_total = 0;
+
+    // Pull the next seed; returns false when the queue is drained.
+    auto fetch = [&]() -> bool {
+        while (true) {
+            const unsigned long long it = atomicAdd(pp.item_counter, 1ull);
+            if (it >= pp.n_items) return false;
+            item = pp.item_ids != nullptr ? pp.item_ids[it] : (uint32_t)it;
+            const float4 a = pp.seeds[2 * (size_t)item];
+            const float4 b = pp.seeds[2 * (size_t)item + 1];
+            const uint32_t batch = item / pp.batch_size;
+            const uint32_t local = item - batch * pp.batch_size;
+            lane_init(s, a, b, pp.batch_rng_seeds[batch], local, pp.seed_offset + item);
+            if (!chunk_alloc(pp, chunk)) {
+                pp.first_chunk[item] = -1;
+                pp.lengths[item] = kOverflowBit;
+                continue;
+            }
+            pp.first_chunk[item] = chunk;
+            fill = 0;
+            emit_point(pp, chunk, fill, a.x, a.y, a.z);
+            return true;
+        }
+    };
+
+    live = fetch();
+    while (live) {
+        bool done = s.n >= p.n_steps;
+        bool overflow = false;
+        if (!done) {
+            float qx, qy, qz;
+            const int r = track_step<MODEL, LMAX, ALGO, CPAD>(p, s, c, qx, qy, qz);
+            if (r == 0) {
+                done = true;
+            } else if (r == 2) {
+                if (emit_point(pp, chunk, fill, qx, qy, qz)) {
+                    s.n++;
+                } else {
+                    done = true;
+                    overflow = true;
+                }
+            }
+        }
+        if (done) {
+            pp.lengths[item] = overflow ? (s.n | kOverflowBit) : s.n;
+            if (!overflow) steps_total += s.steps;
+            live = fetch();
+        }
+    }
+    if (pp.steps_done != nullptr && steps_total != 0) atomicAdd(pp.steps_done, steps_total);
+}
+
+// ----------------------------------------------------------------- gather
+
+__global__ void __launch_bounds__(256) gather_kernel(const float* __restrict__ pool,
+                                                     const int32_t* __restrict__ chunk_next,
+                                                     const int32_t* __restrict__ first_chunk,
+                                                     const uint32_t* __restrict__ lengths,
+                                                     const uint64_t* __restrict__ offsets,
+                                                     const uint32_t* __restrict__ seed_ids, uint32_t n_ids,
+                                                     float* __restrict__ out)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t k = warp; k < n_ids; k += n_warps) {
+        const uint32_t seed = seed_ids[k];
+        int32_t chunk = first_chunk[seed];
+        const uint32_t len = lengths[seed];
+        const uint64_t off = offsets[seed];
+        for (uint32_t base = 0; base < len && chunk >= 0; base += kChunkPoints) {
+            const uint32_t j = base + lane;
+            if (j < len) {
+                const float* src = pool + ((size_t)chunk * kChunkPoints + lane) * 3;
+                float* dst = out + (off + j) * 3;
+                dst[0] = src[0];
+                dst[1] = src[1];
+                dst[2] = src[2];
+            }
+            chunk = chunk_next[chunk];
+        }
+    }
+}
+
+// --------------------------------------------------------------- dispatch
+
+template <template <int, int, int> class Fn, typename... Args>
+cudaError_t dispatch(int model, int lmax, int algo, Args&&... args)
+{
+#define TG_CASE(M, L, A) \
+    if (model == M && (M == kModelDTI || lmax == L) && algo == A) return Fn<M, L, A>::run(args...);
+    TG_CASE(kModelSH, 0, kTransport) TG_CASE(kModelSH, 0, kDiffusion)
+    TG_CASE(kModelSH, 2, kTransport) TG_CASE(kModelSH, 2, kDiffusion)
+    TG_CASE(kModelSH, 4, kTransport) TG_CASE(kModelSH, 4, kDiffusion)
+    TG_CASE(kModelSH, 6, kTransport) TG_CASE(kModelSH, 6, kDiffusion)
+    TG_CASE(kModelSH, 8, kTransport) TG_CASE(kModelSH, 8, kDiffusion)
+    TG_CASE(kModelDTI, 0, kTransport) TG_CASE(kModelDTI, 0, kDiffusion)
+#undef TG_CASE
+    return cudaErrorInvalidValue;
+}
+
+template <int M, int L, int A>
+struct DenseLaunch {
+    static cudaError_t run(const TrackParams& p, const float4* seeds, uint32_t n, uint32_t rng_seed,
+                           uint64_t seed_offset, float4* out, uint32_t* lengths, cudaStream_t stream)
+    {
+        const int block = 128;
+        const int grid = (int)((n + block - 1) / block);
+        track_dense_kernel<M, L, A><<<grid, block, 0, stream>>>(p, seeds, n, rng_seed, seed_offset, out, lengths);
+        return cudaGetLastError();
+    }
+};
+
+template <int M, int L, int A>
+struct PersistentLaunch {
+    static cudaError_t run(const PersistentParams& p, int grid, int block, cudaStream_t stream)
+    {
+        track_persistent_kernel<M, L, A><<<grid, block, 0, stream>>>(p);
+        return cudaGetLastError();
+    }
+};
+
+template <int M, int L, int A>
+struct PersistentOccupancy {
+    static cudaError_t run(int* blocks)
+    {
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, track_persistent_kernel<M, L, A>,
+                                                             persistent_block_size(), 0);
+    }
+};
+
+int lmax_for(uint32_t n_params)
+{
+    int l = 0;
+    while ((uint32_t)n_coef_full(l) < n_params) l += 2;
+    return l;
+}
+
+int persistent_block_size() { return 128; }
+
+int persistent_blocks_per_sm(const FieldDev& f, int algorithm)
+{
+    int blocks = 0;
+    if (dispatch<PersistentOccupancy>(f.model, f.lmax, algorithm, &blocks) != cudaSuccess || blocks < 1)
+        blocks = 1;
+    return blocks;
+}
+
+cudaError_t launch_track_dense(const FieldDev& f, const TrackParams& p, const float4* seeds,
+                               uint32_t n_seeds, uint32_t rng_seed, uint64_t seed_offset, float4* out,
+                               uint32_t* lengths, cudaStream_t stream)
+{
+    if (n_seeds == 0) return cudaSuccess;
+    return dispatch<DenseLaunch>(f.model, f.lmax, p.algorithm, p, seeds, n_seeds, rng_seed, seed_offset,
+                                 out, lengths, stream);
+}
+
+cudaError_t launch_track_persistent(const FieldDev& f, const PersistentParams& p, int grid, int block,
+                                    cudaStream_t stream)
+{
+    if (p.n_items == 0) return cudaSuccess;
+    return dispatch<PersistentLaunch>(f.model, f.lmax, p.t.algorithm, p, grid, block, stream);
+}
+
+cudaError_t launch_gather(const float* pool, const int32_t* chunk_next, const int32_t* first_chunk,
+                          const uint32_t* lengths, const uint64_t* offsets, const uint32_t* seed_ids,
+                          uint32_t n_ids, float* out_points, cudaStream_t stream)
+{
+    if (n_ids == 0) return cudaSuccess;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int block = 256;
+    const uint64_t threads = (uint64_t)n_ids * 32u;
+    uint64_t grid = (threads + block - 1) / block;
+    if (grid > (uint64_t)sms * 16) grid = (uint64_t)sms * 16;
+    gather_kernel<<<(int)grid, block, 0, stream>>>(pool, chunk_next, first_chunk, lengths, offsets, seed_ids,
+                                                   n_ids, out_points);
+    return cudaGetLastError();
+}
+
+}  // namespace tg

@@ -1,0 +1,162 @@
+"""Low-level streamline tracking (reference ``tractography/tracking.py:22-178``).
+
+``tractogram()`` keeps the reference's signature and semantics: every seed
+is advanced by the algorithm while it stays inside the domain and the field
+can be evaluated; a point is recorded every ``save_at`` of path length
+(back-interpolated to the exact save position), the seed itself first, up
+to ``floor(maximum_streamline_length / save_at)`` points.
+
+Execution differs from the reference: no source assembly or per-call
+compilation, the field and domain stay resident on the device, and seeds are
+tracked by the persistent kernel whose packed output is copied back once.
+``tractogram_dense()`` runs the one-thread-per-seed kernel with the
+reference's dense output layout.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .algorithm import BaseAlgorithm, to_struct
+from .domain import BaseDomain
+from .domain import Image as ImageDomain
+from .field import BaseField
+from .field import Image as ImageField
+from .local import model_id
+from .seeds import validate_seed_array
+from .streamlines import ArraySequence, Tractogram
+
+
+class TrackResult:
+    """Packed output of one tracker run."""
+
+    def __init__(self, points, offsets, lengths, steps):
+        self.points = points
+        self.offsets = offsets
+        self.lengths = lengths
+        self.steps = int(steps)
+
+    def streamlines(self, keep=None) -> ArraySequence:
+        if keep is None:
+            return ArraySequence(self.points, self.offsets, self.lengths)
+        return ArraySequence(self.points, self.offsets[keep], self.lengths[keep])
+
+
+def _check_compatible(algorithm: BaseAlgorithm, field: BaseField) -> None:
+    if algorithm.local_model.n_parameters != field.n_parameters:
+        raise ValueError(
+            "Incompatible local model and field, they do not have the "
+            "same number of parameters: "
+            f"{algorithm.local_model.n_parameters} != {field.n_parameters}"
+        )
+
+
+def _n_steps(save_at: float, maximum_streamline_length: float) -> int:
+    n_steps = int(np.floor(maximum_streamline_length / save_at))
+    if n_steps <= 0:
+        # The reference allocates an empty point buffer here and fails
+        # (opencl.py:323-324).
+        raise ValueError("nbytes must be positive.")
+    return n_steps
+
+
+def _handles(algorithm, domain, field, runtime):
+    if not isinstance(domain, ImageDomain):
+        raise NotImplementedError(f"{type(domain).__name__} has no compiled CUDA code path")
+    if not isinstance(field, ImageField):
+        raise NotImplementedError(f"{type(field).__name__} has no compiled CUDA code path")
+    mid = model_id(algorithm.local_model)
+    return domain.device(runtime), field.device(runtime, mid)
+
+
+def track_packed(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, seeds: np.ndarray, *,
+                 save_at: float, n_steps: int, batch_size: int, batch_rng_seeds, runtime,
+                 philox_key: int = 0, seed_offset: int = 0) -> TrackResult:
+    """Track all seeds with one persistent-tracker run.
+
+    Seed ``i`` is tracked with the stream of batch ``i // batch_size``
+    (seed ``batch_rng_seeds[b]``) and stream id ``i % batch_size``.
+    """
+    n = int(seeds.shape[0])
+    batch_rng_seeds = np.ascontiguousarray(batch_rng_seeds, dtype=np.uint32)
+    if len(batch_rng_seeds) != (n + batch_size - 1) // batch_size:
+        raise ValueError("one rng seed per batch is required")
+    lengths = np.empty(n, dtype=np.uint32)
+    offsets = np.empty(n, dtype=np.uint64)
+    total = ctypes.c_uint64()
+    steps = ctypes.c_uint64()
+    with runtime.device_scope():
+        d_handle, f_handle = _handles(algorithm, domain, field, runtime)
+        a = to_struct(algorithm, 0, philox_key, seed_offset)
+        seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+        _lib.check(runtime.lib.tg_tracker_run(
+            runtime.tracker(), ctypes.byref(a), d_handle, f_handle, seeds.ctypes.data_as(ctypes.c_void_p), 1, n,
+            int(batch_size), batch_rng_seeds.ctypes.data_as(ctypes.c_void_p), float(save_at), int(n_steps),
+            lengths.ctypes.data_as(ctypes.c_void_p), offsets.ctypes.data_as(ctypes.c_void_p),
+            ctypes.byref(total), ctypes.byref(steps), ctypes.c_void_p(runtime.stream_handle)))
+        points = runtime.pinned((int(total.value), 3), np.float32) if total.value else np.empty((0, 3), np.float32)
+        if total.value:
+            _lib.check(runtime.lib.tg_tracker_copy_points(
+                runtime.tracker(), points.ctypes.data_as(ctypes.c_void_p), 0, total.value, 1,
+                ctypes.c_void_p(runtime.stream_handle)))
+    return TrackResult(points, offsets.astype(np.int64), lengths.astype(np.int64), steps.value)
+
+
+def tractogram(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, seeds: np.ndarray,
+               save_at: float = 1.0, maximum_streamline_length: float = 300.0, runtime=None) -> Tractogram:
+    """Track streamlines from (n, 8) position-and-orientation seeds.
+
+    Raises:
+        ValueError: if the local model and field have different parameter
+            counts (tracking.py:72-78).
+    """
+    seeds = validate_seed_array(seeds)
+    _check_compatible(algorithm, field)
+    n_seeds = seeds.shape[0]
+    if n_seeds == 0:
+        return Tractogram([], affine_to_rasmm=np.eye(4))
+    from .runtime import default_runtime
+
+    runtime = runtime or default_runtime()
+    n_steps = _n_steps(save_at, maximum_streamline_length)
+    rng_seed = algorithm.get_rng_seed()
+    key = algorithm.philox_key() if algorithm.rng_mode() == _lib.RNG_PHILOX else 0
+    result = track_packed(algorithm, domain, field, seeds, save_at=save_at, n_steps=n_steps, batch_size=n_seeds,
+                          batch_rng_seeds=[rng_seed], runtime=runtime, philox_key=key)
+    return Tractogram(result.streamlines(), affine_to_rasmm=np.eye(4))
+
+
+def tractogram_dense(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, seeds: np.ndarray,
+                     save_at: float = 1.0, maximum_streamline_length: float = 300.0, runtime=None,
+                     rng_seed: int | None = None, philox_key: int | None = None):
+    """The reference kernel contract: dense (n, n_steps, 4) points and lengths.
+
+    Runs one thread per seed (the plain one-launch form) and returns the
+    host arrays the reference's kernel writes (tracking.py:152-176).
+    """
+    seeds = validate_seed_array(seeds)
+    _check_compatible(algorithm, field)
+    n = seeds.shape[0]
+    from .runtime import default_runtime
+
+    runtime = runtime or default_runtime()
+    n_steps = _n_steps(save_at, maximum_streamline_length)
+    if rng_seed is None:
+        rng_seed = algorithm.get_rng_seed()
+    if philox_key is None:
+        philox_key = algorithm.philox_key() if algorithm.rng_mode() == _lib.RNG_PHILOX else 0
+    out = np.zeros((n, n_steps, 4), dtype=np.float32)
+    lengths = np.zeros(n, dtype=np.uint32)
+    if n == 0:
+        return out, lengths
+    with runtime.device_scope():
+        d_handle, f_handle = _handles(algorithm, domain, field, runtime)
+        a = to_struct(algorithm, rng_seed, philox_key, 0)
+        _lib.check(runtime.lib.tg_tractogram_host(
+            ctypes.byref(a), d_handle, f_handle, seeds.ctypes.data_as(ctypes.c_void_p), n, float(save_at), n_steps,
+            out.ctypes.data_as(ctypes.c_void_p), lengths.ctypes.data_as(ctypes.c_void_p),
+            ctypes.c_void_p(runtime.stream_handle)))
+    return out, lengths
