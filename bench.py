@@ -5,9 +5,12 @@ Workload (single GPU): the plain Diffusion configuration -- a synthetic
 145 x 174 x 145 spherical-harmonic FOD (lmax 8, 45 float32 coefficients,
 1.25 mm voxels, about 660 MB), seeds drawn by ``seeds.from_fod`` with a
 fixed NumPy seed, Diffusion with step 0.001 mm, gamma 1, noise variance 0.1,
-save_at 0.25 mm, maximum length 300 mm, batches of 50 000 seeds.  One
-benchmark step is one batch: the reference's unit of work, one
-``tracking.tractogram`` call.
+save_at 0.25 mm, maximum length 300 mm, 1 000 000 seeds in batches of
+50 000.  One benchmark step is the whole job, i.e. one
+``tg.tractogram(fod, seeds, algorithm=..., batch_size=50000)`` call: every
+batch keeps its own reference RNG seed and stream ids, and all batches run
+in one persistent launch (a 50 000-seed batch alone cannot fill the ~95 000
+resident lanes of a B200).
 
 Metric: streamline-steps/s, where a step is one iteration of the tracking
 loop that passed both the domain and the field check (tracking.py:121-147).
@@ -62,16 +65,17 @@ NOISE = 0.1
 BYTES_PER_STEP = 4 * C + 4 + 16 * STEP / SAVE_AT
 WORKLOAD = ("config1 Diffusion: SH lmax 8 (45 f32 coefficients) 145x174x145 at 1.25 mm, 3 bundles; "
             "seeds from seeds.from_fod; step 0.001 mm, gamma 1, noise_variance 0.1; save_at 0.25, "
-            "max length 300 mm; batch 50000 seeds per step")
+            "max length 300 mm; 1M seeds per step in reference batches of 50000")
 
 
 def parse_args():
     p = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--batch", type=int, default=50000)
+    p.add_argument("--seeds", type=int, default=1000000, help="seeds per step (one tg.tractogram job)")
+    p.add_argument("--batch", type=int, default=50000, help="reference batch_size inside a job")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
@@ -196,11 +200,13 @@ def run_ours(args):
     torch.cuda.set_device(local_rank)
     runtime = tg.CudaRuntime(local_rank)
     lib = runtime.lib
-    n_total = args.batch * (args.warmup + args.steps)
-    fod, field, domain, seeds, algorithm = setup_workload(rank, n_total, runtime)
+    n_job = args.seeds
+    fod, field, domain, seeds, algorithm = setup_workload(rank, n_job, runtime)
     n_steps = int(math.floor(MAX_LENGTH / SAVE_AT))
-    batches = [np.ascontiguousarray(seeds[i * args.batch:(i + 1) * args.batch]) for i in range(args.warmup + args.steps)]
-    rng_seeds = [np.array([algorithm.get_rng_seed()], dtype=np.uint32) for _ in batches]
+    n_batches = (n_job + args.batch - 1) // args.batch
+    # one reference RNG seed per batch, drawn in batch order for every job
+    rng_seeds = [np.array([algorithm.get_rng_seed() for _ in range(n_batches)], dtype=np.uint32)
+                 for _ in range(args.warmup + args.steps)]
     stream = runtime.stream
     sh = ctypes.c_void_p(runtime.stream_handle)
     with runtime.device_scope():
@@ -208,15 +214,12 @@ def run_ours(args):
         f_handle = field.device(runtime, _lib.MODEL_SH)
         tracker = runtime.tracker()
         a = to_struct(algorithm)
-        dev_batches = [runtime.to_device(b) for b in batches]
-        host_batches = []
-        for b in batches:
-            pb = runtime.pinned(b.shape, np.float32)
-            pb[...] = b
-            host_batches.append(pb)
+        dev_seeds = runtime.to_device(seeds)
+        host_seeds = runtime.pinned(seeds.shape, np.float32)
+        host_seeds[...] = seeds
         torch.cuda.synchronize()
-        lengths = np.empty(args.batch, np.uint32)
-        offsets = np.empty(args.batch, np.uint64)
+        lengths = np.empty(n_job, np.uint32)
+        offsets = np.empty(n_job, np.uint64)
         total = ctypes.c_uint64()
         steps = ctypes.c_uint64()
         kms = ctypes.c_float()
@@ -224,20 +227,19 @@ def run_ours(args):
         launches = ctypes.c_uint32()
 
         def run(i, on_host):
-            src = host_batches[i] if on_host else dev_batches[i]
-            ptr = src.ctypes.data_as(ctypes.c_void_p) if on_host else ctypes.c_void_p(src.data_ptr())
+            ptr = host_seeds.ctypes.data_as(ctypes.c_void_p) if on_host else ctypes.c_void_p(dev_seeds.data_ptr())
             _lib.check(lib.tg_tracker_run(
-                tracker, ctypes.byref(a), d_handle, f_handle, ptr, 1 if on_host else 0, args.batch, args.batch,
+                tracker, ctypes.byref(a), d_handle, f_handle, ptr, 1 if on_host else 0, n_job, args.batch,
                 rng_seeds[i].ctypes.data_as(ctypes.c_void_p), SAVE_AT, n_steps,
                 lengths.ctypes.data_as(ctypes.c_void_p), offsets.ctypes.data_as(ctypes.c_void_p),
                 ctypes.byref(total), ctypes.byref(steps), sh))
             _lib.check(lib.tg_tracker_stats(tracker, ctypes.byref(kms), ctypes.byref(waves), ctypes.byref(launches)))
             return int(steps.value), int(total.value), float(kms.value), int(launches.value), int(waves.value)
 
-        out_host = runtime.pinned((args.batch * n_steps, 3), np.float32)
-
+        warm_points = 0
         for i in range(args.warmup):
-            run(i, on_host=False)
+            warm_points = max(warm_points, run(i, on_host=False)[1])
+        out_host = runtime.pinned((int(warm_points * 1.25) + 1024, 3), np.float32)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
         sampler = ClockSampler(local_rank)
@@ -269,10 +271,12 @@ def run_ours(args):
             h2d = d2h = 0
             for i in range(args.warmup, args.warmup + args.steps):
                 s, p, _, _, _ = run(i, on_host=True)
+                if p > out_host.shape[0]:
+                    out_host = runtime.pinned((p, 3), np.float32)
                 _lib.check(lib.tg_tracker_copy_points(tracker, out_host.ctypes.data_as(ctypes.c_void_p), 0, p, 1, sh))
                 e2e_steps += s
-                h2d += batches[i].nbytes + 4
-                d2h += p * 12 + args.batch * (4 + 8)
+                h2d += seeds.nbytes + rng_seeds[i].nbytes
+                d2h += p * 12 + n_job * (4 + 8)
             ev1.record(stream)
             torch.cuda.synchronize()
             e2e_ms = ev0.elapsed_time(ev1)
@@ -311,13 +315,14 @@ def run_ours(args):
         "data": "synthetic (seeded generator; no dataset)",
         "config": {
             "workload": WORKLOAD,
-            "batch_seeds": args.batch,
+            "seeds_per_step": n_job,
+            "batch_size": args.batch,
             "max_points_per_streamline": n_steps,
             "cache": "inputs larger than L2: 660 MB FOD volume, 126 MB L2",
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "rng": "MWC64X reference stream per batch",
         },
-        "streamlines_per_s": args.batch * args.steps * world / (dev_ms / 1e3),
+        "streamlines_per_s": n_job * args.steps * world / (dev_ms / 1e3),
         "points_per_step": dev_points / args.steps / max(1, world),
         "e2e": {
             "value": e2e_steps / (e2e_ms / 1e3),
@@ -340,7 +345,7 @@ def run_ours(args):
         "clocks": sampler.summary(),
     }
     if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(field, domain, seeds[args.warmup * args.batch:])
+        line["cpu_baseline"] = cpu_baseline(field, domain, seeds)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
