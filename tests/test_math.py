@@ -1,0 +1,82 @@
+"""Accuracy of the shared binary32 math layer and of the SH basis (CPU, through the oracle).
+
+The math layer (csrc/tg_fmath.h) must stay within 2 ulp of double-precision
+libm; the oracle's table-driven SH evaluation must match the float64 SciPy
+basis (core.ishtmtx, the reference's core.py:36-69 convention) to float32
+rounding.
+"""
+
+import numpy as np
+import pytest
+
+import tractography_b200 as tg
+
+
+def ulp_error(got, want):
+    got = np.asarray(got, dtype=np.float64)
+    want32 = np.asarray(want, dtype=np.float32)
+    spacing = np.abs(np.spacing(want32)).astype(np.float64)
+    spacing[spacing == 0] = np.finfo(np.float32).smallest_subnormal
+    return np.abs(got - np.asarray(want, dtype=np.float64)) / spacing
+
+
+@pytest.mark.parametrize("fn", ["sin", "cos"])
+def test_sincos_within_two_ulp(oracle, fn):
+    x = np.linspace(-100.0, 100.0, 2_000_001, dtype=np.float32)
+    got = oracle.math(fn, x)
+    want = getattr(np, fn)(x.astype(np.float64))
+    err = ulp_error(got, want)
+    assert err.max() <= 2.0, (fn, float(err.max()), x[np.argmax(err)])
+
+
+def test_exp_within_two_ulp(oracle):
+    x = np.linspace(-103.0, 88.7, 2_000_001, dtype=np.float32)
+    err = ulp_error(oracle.math("exp", x), np.exp(x.astype(np.float64)))
+    assert err.max() <= 2.0
+    special = oracle.math("exp", np.array([0.0, -200.0, 200.0, np.nan], np.float32))
+    assert special[0] == 1.0 and special[1] == 0.0 and np.isinf(special[2]) and np.isnan(special[3])
+
+
+def test_log_within_two_ulp(oracle):
+    rng = np.random.default_rng(0)
+    x = np.concatenate([
+        np.linspace(0.5, 2.0, 1_000_001, dtype=np.float32),
+        (2.0 ** rng.uniform(-140, 127, 1_000_000)).astype(np.float32),
+    ])
+    x = x[x > 0]
+    err = ulp_error(oracle.math("log", x), np.log(x.astype(np.float64)))
+    assert err.max() <= 2.0
+    special = oracle.math("log", np.array([1.0, 0.0, -1.0, np.inf], np.float32))
+    assert special[0] == 0.0 and special[1] == -np.inf and np.isnan(special[2]) and special[3] == np.inf
+
+
+@pytest.mark.parametrize("C", [1, 6, 15, 28, 45])
+def test_oracle_sh_basis_matches_scipy(oracle, C):
+    rng = np.random.default_rng(C)
+    n = 4000
+    phi = rng.uniform(0, 2 * np.pi, n)
+    theta = np.arccos(rng.uniform(-1, 1, n))
+    o = np.stack(tg.core.sph2cart(phi, theta, 1.0), -1).astype(np.float32)
+    params = (rng.normal(size=(n, C)) * 0.1).astype(np.float32)
+    params[:, 0] = 40.0                     # softplus is the identity above 0.3
+    got = oracle.local_evaluate(oracle.MODEL_SH, params, o)
+    want = tg.local.RealSymmetricSphericalHarmonics(C).evaluate(params.astype(np.float64), o.astype(np.float64))
+    scale = np.abs(want).max(axis=0)
+    assert np.all(np.abs(got - want).max(axis=0) <= 5e-6 * scale + 1e-6)
+
+
+def test_oracle_dti_matches_float64(oracle):
+    rng = np.random.default_rng(1)
+    p = rng.normal(size=(500, 6)).astype(np.float32)
+    o = rng.normal(size=(500, 3)).astype(np.float32)
+    o /= np.linalg.norm(o, axis=1, keepdims=True)
+    got = oracle.local_evaluate(oracle.MODEL_DTI, p, o)
+    want = tg.local.DiffusionTensorImaging().evaluate(p.astype(np.float64), o.astype(np.float64))
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-5)
+
+
+def test_philox_known_answer(oracle):
+    # Random123 known-answer vectors for philox4x32-10 (Salmon et al. 2011)
+    assert list(oracle.philox([0, 0, 0, 0], [0, 0])) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert list(oracle.philox([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2)) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6,
+                                                                      0x6D5451FD]
