@@ -141,6 +141,30 @@ int tg_tracker_stats(const tg_tracker* tracker, float* kernel_ms, uint32_t* wave
 int tg_tracker_copy_points(tg_tracker* tracker, float* dst, uint64_t first, uint64_t count,
                            int dst_on_host, void* stream);
 
+/* Largest number of batches one tg_tractogram_noalloc call accepts. */
+#define TG_NOALLOC_MAX_BATCHES 16384
+
+/* Tracking for callers that cannot allow the library to allocate device
+ * memory (for example a host application that owns the GPU memory budget and
+ * hands fixed buffers to plugins, or a loop where cudaMalloc's possible device
+ * synchronisation is unacceptable).  No counterpart in the reference: it is
+ * tg_tractogram's dense contract run by the persistent lane-refill tracker
+ * over batches (as tg_tracker_run numbers them: batch b = seeds
+ * [b * batch_size, (b + 1) * batch_size) with seed batch_rng_seeds[b], a host
+ * array), writing into the caller's device buffers `streamlines`
+ * (n_seeds, n_steps, 4) and `lengths` (n_seeds).  It calls no cudaMalloc,
+ * cudaFree or allocating library routine; its only scratch is a library-wide
+ * static device array of 64 KiB + 256 B per GPU (held until process exit)
+ * that holds at most TG_NOALLOC_MAX_BATCHES batch seeds -- more batches are
+ * rejected with TG_ERR_INVALID_ARGUMENT.  The first call on a device looks
+ * up that array's address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Every call shares the array: calls that overlap on the
+ * GPU race and must be serialised by the caller. */
+int tg_tractogram_noalloc(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
+                          const float* seeds, uint32_t n_seeds, uint32_t batch_size,
+                          const uint32_t* batch_rng_seeds, float save_at, uint32_t n_steps, float* streamlines,
+                          uint32_t* lengths, void* stream);
+
 /* FOD seeding: seeds.cl:99-118 as launched by seeds.py:174-216.  `fod` is
  * the device sparse (nnz, n_coefficients) array, `voxels` the device
  * (nnz, 4) voxel indices with w = 1, `affine` the device voxel-to-world

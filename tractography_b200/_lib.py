@@ -37,6 +37,7 @@ EXPORTS = (
     "tg_domain_destroy",
     "tg_tractogram",
     "tg_tractogram_host",
+    "tg_tractogram_noalloc",
     "tg_tracker_create",
     "tg_tracker_destroy",
     "tg_tracker_run",
@@ -102,6 +103,7 @@ def load() -> ctypes.CDLL:
         "tg_domain_destroy": ([P], ctypes.c_int),
         "tg_tractogram": ([AP, P, P, P, U32, F, U32, P, P, P], ctypes.c_int),
         "tg_tractogram_host": ([AP, P, P, P, U32, F, U32, P, P, P], ctypes.c_int),
+        "tg_tractogram_noalloc": ([AP, P, P, P, U32, U32, P, F, U32, P, P, P], ctypes.c_int),
         "tg_tracker_create": ([U64, ctypes.POINTER(P)], ctypes.c_int),
         "tg_tracker_destroy": ([P], ctypes.c_int),
         "tg_tracker_run": ([P, AP, P, P, P, ctypes.c_int, U32, U32, P, F, U32, P, P,

@@ -171,6 +171,23 @@ int sm_count()
 
 }  // namespace
 
+namespace tg {
+
+// Used by tg_noalloc.cu, which cannot see the handle layouts.
+int track_params_from_handles(const tg_algorithm* a, const tg_domain* d, const tg_field* f, float save_at,
+                              uint32_t n_steps, TrackParams* out, int* model, int* lmax)
+{
+    const int st = make_track_params(a, d, f, save_at, n_steps, out);
+    if (st != TG_OK) return st;
+    *model = f->d.model;
+    *lmax = f->d.lmax;
+    return TG_OK;
+}
+
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+
+}  // namespace tg
+
 extern "C" {
 
 int tg_abi_version(void) { return TG_ABI_VERSION; }
