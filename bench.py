@@ -77,6 +77,9 @@ def parse_args():
     p.add_argument("--seeds", type=int, default=1000000, help="seeds per step (one tg.tractogram job)")
     p.add_argument("--batch", type=int, default=50000, help="reference batch_size inside a job")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=["config1", "mixed"], default="config1",
+                   help="config1 (default headline) or the 64-job mixed workload")
+    p.add_argument("--jobs", type=int, default=64, help="jobs of the mixed workload")
     return p.parse_args()
 
 
@@ -440,10 +443,152 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def build_mixed_jobs(n_jobs, seed=0):
+    """Config-3 jobs (see synthetic.mixed_job_specs); volumes shared per (size, lmax)."""
+    import tractography_b200 as tg
+    from tractography_b200 import jobs as jobs_module
+    from tractography_b200 import synthetic
+
+    cache = {}
+    out = []
+    for sp in synthetic.mixed_job_specs(n_jobs=n_jobs, seed=seed):
+        key = (sp["shape"], sp["lmax"])
+        if key not in cache:
+            fod, mask = synthetic.bundle_field(sp["shape"], lmax=sp["lmax"], seed=len(cache))
+            cache[key] = (tg.field.Image(fod), tg.domain.Image(mask), mask)
+        field, domain, mask = cache[key]
+        C = (sp["lmax"] + 1) * (sp["lmax"] + 2) // 2
+        model = tg.local.RealSymmetricSphericalHarmonics(C)
+        step = 0.2   # 0.1 voxel at 2 mm
+        if sp["algorithm"] == "transport":
+            alg = tg.algorithm.Transport(model, step_size=step, gamma=1.0)
+        else:
+            alg = tg.algorithm.Diffusion(model, step_size=step, gamma=1.0, noise_variance=sp["noise_variance"],
+                                         seed=sp["seed"])
+        seeds = synthetic.uniform_seeds(mask, sp["n_seeds"], seed=sp["seed"])
+        batch = 50000
+        n_batches = (len(seeds) + batch - 1) // batch
+        rng = np.array([alg.get_rng_seed() for _ in range(n_batches)], dtype=np.uint32)
+        out.append(jobs_module.Job(field=field, domain=domain, algorithm=alg, seeds=seeds, save_at=SAVE_AT,
+                                   n_steps=int(math.floor(sp["max_length"] / SAVE_AT)), min_points=0,
+                                   batch_size=batch, batch_rng_seeds=rng))
+    return out
+
+
+def run_mixed(args):
+    """Config 3: 64 uneven jobs, persistent multi-job run vs plain one launch per batch."""
+    import torch
+
+    import tractography_b200 as tg
+    from tractography_b200 import _lib, tracking
+    from tractography_b200.algorithm import to_struct
+
+    torch.cuda.set_device(0)
+    runtime = tg.CudaRuntime(0)
+    lib = runtime.lib
+    sh = ctypes.c_void_p(runtime.stream_handle)
+    jobs = build_mixed_jobs(args.jobs)
+    n_total = sum(j.n_seeds for j in jobs)
+    with runtime.device_scope():
+        structs = (_lib.Job * len(jobs))()
+        dev_seeds = []
+        for k, job in enumerate(jobs):
+            d_h, f_h = tracking._handles(job.algorithm, job.domain, job.field, runtime)
+            ds = runtime.to_device(job.seeds)
+            dev_seeds.append(ds)
+            s = structs[k]
+            s.domain, s.field = d_h, f_h
+            s.algorithm = to_struct(job.algorithm)
+            s.seeds = ds.data_ptr()
+            s.n_seeds = job.n_seeds
+            s.batch_size = job.batch_size
+            s.batch_rng_seeds = job.batch_rng_seeds.ctypes.data
+            s.save_at = job.save_at
+            s.n_steps = job.n_steps
+        lengths = np.empty(n_total, np.uint32)
+        offsets = np.empty(n_total, np.uint64)
+        total, steps = ctypes.c_uint64(), ctypes.c_uint64()
+        kms, waves, launches = ctypes.c_float(), ctypes.c_uint32(), ctypes.c_uint32()
+
+        def persistent():
+            _lib.check(lib.tg_tracker_run_jobs(runtime.tracker(), structs, len(jobs), 0,
+                                               lengths.ctypes.data_as(ctypes.c_void_p),
+                                               offsets.ctypes.data_as(ctypes.c_void_p), ctypes.byref(total),
+                                               ctypes.byref(steps), sh))
+            _lib.check(lib.tg_tracker_stats(runtime.tracker(), ctypes.byref(kms), ctypes.byref(waves),
+                                            ctypes.byref(launches)))
+
+        max_batch = max(min(j.batch_size, j.n_seeds) for j in jobs)
+        max_steps = max(j.n_steps for j in jobs)
+        d_out = torch.empty((max_batch * max_steps * 4,), dtype=torch.float32, device=runtime.device)
+        d_len = torch.empty((n_total,), dtype=torch.int32, device=runtime.device)
+
+        def plain():
+            n_launch = 0
+            base = 0
+            for k, job in enumerate(jobs):
+                d_h, f_h = tracking._handles(job.algorithm, job.domain, job.field, runtime)
+                for b in range(len(job.batch_rng_seeds)):
+                    lo = b * job.batch_size
+                    n = min(job.batch_size, job.n_seeds - lo)
+                    a = to_struct(job.algorithm, int(job.batch_rng_seeds[b]))
+                    _lib.check(lib.tg_tractogram(ctypes.byref(a), d_h, f_h,
+                                                 ctypes.c_void_p(dev_seeds[k].data_ptr() + lo * 32), n,
+                                                 job.save_at, job.n_steps, ctypes.c_void_p(d_out.data_ptr()),
+                                                 ctypes.c_void_p(d_len.data_ptr() + 4 * (base + lo)), sh))
+                    n_launch += 1
+                base += job.n_seeds
+            return n_launch
+
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(args.warmup):
+            persistent()
+            plain()
+        torch.cuda.synchronize()
+        p_ms = q_ms = 0.0
+        n_plain = 0
+        for _ in range(args.steps):
+            ev0.record(runtime.stream)
+            persistent()
+            ev1.record(runtime.stream)
+            torch.cuda.synchronize()
+            p_ms += ev0.elapsed_time(ev1)
+            ev0.record(runtime.stream)
+            n_plain = plain()
+            ev1.record(runtime.stream)
+            torch.cuda.synchronize()
+            q_ms += ev0.elapsed_time(ev1)
+        plain_len = d_len.cpu().numpy().view(np.uint32)
+    work = int(steps.value)
+    line = {
+        "metric": METRIC, "workload": "mixed", "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded generator; no dataset)",
+        "value": work / (p_ms / args.steps / 1e3),
+        "plain_value": work / (q_ms / args.steps / 1e3),
+        "speedup_vs_plain": q_ms / p_ms,
+        "ms_per_step": p_ms / args.steps,
+        "plain_ms_per_step": q_ms / args.steps,
+        "gpu_launches_per_step": int(launches.value),
+        "plain_launches_per_step": n_plain,
+        "identical_lengths": bool(np.array_equal(plain_len, lengths)),
+        "config": {
+            "workload": ("64 jobs: volume 64^3 / 96x96x60 / 128^3 / 145x174x145, SH lmax 4/6/8, seeds "
+                         "log-U[1k, 500k], Transport or Diffusion (noise U[0.05, 0.2]), max length "
+                         "U[50, 300] mm, step 0.2 mm (0.1 voxel), save_at 0.25, batch 50000"),
+            "jobs": len(jobs), "seeds": n_total, "steps_per_run": work,
+            "plain": "one tg_tractogram launch per 50000-seed batch, jobs in order, dense output",
+        },
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "mixed":
+        run_mixed(args)
     else:
         run_ours(args)
 

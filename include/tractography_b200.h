@@ -130,6 +130,32 @@ int tg_tracker_run(tg_tracker* tracker, const tg_algorithm* algorithm, const tg_
                    uint32_t n_steps, uint32_t* h_lengths, uint64_t* h_offsets,
                    uint64_t* total_points, uint64_t* total_steps, void* stream);
 
+/* One tracking job: the arguments of one reference tg.tractogram call
+ * (tractography/__init__.py:369-540) after its host-side preparation. */
+typedef struct {
+    const tg_domain* domain;
+    const tg_field* field;
+    tg_algorithm algorithm;          /* rng_seed unused: see batch_rng_seeds */
+    const float* seeds;              /* (n_seeds, 8); host or device, see seeds_on_host */
+    uint32_t n_seeds;
+    uint32_t batch_size;
+    const uint32_t* batch_rng_seeds; /* host, ceil(n_seeds / batch_size) seeds */
+    float save_at;
+    uint32_t n_steps;
+} tg_job;
+
+/* Track many jobs of uneven size, model, algorithm and length at once: every
+ * job's seeds go to a device queue of its code path (model, lmax,
+ * algorithm); one persistent launch per code path, all on concurrent
+ * streams, drains the queues with lanes refilling as streamlines terminate.
+ * Outputs are over the concatenation of the jobs' seeds in the order given:
+ * h_lengths and h_offsets have sum(n_seeds) entries; points are read with
+ * tg_tracker_copy_points.  Results equal those of one tg_tracker_run per
+ * job.  No reference counterpart: the reference runs jobs one after another. */
+int tg_tracker_run_jobs(tg_tracker* tracker, const tg_job* jobs, uint32_t n_jobs, int seeds_on_host,
+                        uint32_t* h_lengths, uint64_t* h_offsets, uint64_t* total_points,
+                        uint64_t* total_steps, void* stream);
+
 /* Statistics of the last tg_tracker_run: device time of the tracking
  * kernel launches (CUDA events on the run's stream), number of waves (more
  * than one only when the point pool ran out) and number of kernel launches.

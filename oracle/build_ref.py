@@ -1,0 +1,247 @@
+#!/usr/bin/env python3
+"""Build oracle/_ref/libtgref.so: the reference's own tracking kernels on the CPU.
+
+Test infrastructure only.  For each (model, coefficient count, algorithm)
+combination this script lets the reference assemble its `tractogram` kernel
+exactly as it does before launching it (tractography/tracking.py:92-173):
+it calls the reference's ``tracking.tractogram`` with a recording runtime
+whose ``build_program`` keeps the source instead of compiling it.  The
+source is then made C++: the reference's ``#include``d kernel files are
+inlined from the reference tree, OpenCL vector literals ``(float4)(...)``
+and ``(T){...}`` become ``make_T(...)`` calls, the templated point budget
+becomes a run-time value, and one counter increment is inserted before the
+orientation update so accepted steps can be counted.  oracle/clshim.hpp
+supplies the OpenCL built-ins.  g++ compiles each variant in its own
+translation unit and namespace; the outputs go only to oracle/_ref/.
+
+Nothing from the reference is copied into this repository: the sources are
+read from the reference tree at build time.
+
+Usage: python oracle/build_ref.py [--reference /root/reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import os
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+N_STEPS_SENTINEL = 987654
+
+VARIANTS = [
+    # name, model, coefficients, algorithm
+    ("sh15_transport", "sh", 15, "transport"),
+    ("sh15_diffusion", "sh", 15, "diffusion"),
+    ("sh28_transport", "sh", 28, "transport"),
+    ("sh28_diffusion", "sh", 28, "diffusion"),
+    ("sh45_transport", "sh", 45, "transport"),
+    ("sh45_diffusion", "sh", 45, "diffusion"),
+    ("dti_transport", "dti", 6, "transport"),
+    ("dti_diffusion", "dti", 6, "diffusion"),
+]
+
+
+class _Captured(Exception):
+    pass
+
+
+class RecordingRuntime:
+    """Stands in for OpenCLRuntime: records the program source, runs nothing."""
+
+    def __init__(self):
+        self.source = None
+
+    def buffer_from_array(self, data, access=None):
+        return np.ascontiguousarray(data)
+
+    def allocate_buffer(self, nbytes, access=None):
+        return nbytes
+
+    def build_program(self, source, options=()):
+        self.source = source
+        raise _Captured()
+
+
+def capture(ref, model, n_coefficients, algorithm):
+    Image = sys.modules["nibabel.nifti1"].Nifti1Image
+    field = ref.field.Image(Image(np.ones((2, 2, 2, n_coefficients), np.float32), np.eye(4)))
+    domain = ref.domain.Image(Image(np.ones((2, 2, 2), np.uint8), np.eye(4)))
+    local = ref.local.DiffusionTensorImaging() if model == "dti" else \
+        ref.local.RealSymmetricSphericalHarmonics(n_coefficients)
+    alg = ref.algorithm.Transport(local) if algorithm == "transport" else ref.algorithm.Diffusion(local)
+    seeds = np.array([[0, 0, 0, 1, 1, 0, 0, 0]], np.float32)
+    rt = RecordingRuntime()
+    try:
+        ref.tracking.tractogram(alg, domain, field, seeds, save_at=1.0,
+                                maximum_streamline_length=float(N_STEPS_SENTINEL), runtime=rt)
+    except _Captured:
+        return rt.source
+    raise RuntimeError("the reference did not build a program")
+
+
+def capture_update(ref, model, n_coefficients, algorithm):
+    """The reference's standalone orientation-update kernel (algorithm.py:701-790)."""
+    local = ref.local.DiffusionTensorImaging() if model == "dti" else \
+        ref.local.RealSymmetricSphericalHarmonics(n_coefficients)
+    alg = ref.algorithm.Transport(local) if algorithm == "transport" else ref.algorithm.Diffusion(local)
+    rt = RecordingRuntime()
+    try:
+        ref.algorithm.update_orientation(alg, np.zeros((1, n_coefficients)), np.array([[0.0, 0.0, 1.0]]), runtime=rt)
+    except _Captured:
+        return rt.source
+    raise RuntimeError("the reference did not build a program")
+
+
+def inline_includes(text, kernel_dir, seen=None):
+    seen = set() if seen is None else seen
+
+    def repl(m):
+        path = kernel_dir / m.group(1)
+        if path in seen:
+            return ""
+        seen.add(path)
+        return inline_includes(path.read_text(), kernel_dir, seen)
+
+    return re.sub(r'#include\s+"([^"]+)"', repl, text)
+
+
+def rewrite_literals(text):
+    # (T)(...)  ->  make_T(...)
+    text = re.sub(r"\((float|int|uint)([234])\)\s*\(", r"make_\1\2(", text)
+    # (T){...}  ->  make_T(...) for vectors, T{...} for structs
+    out = []
+    i = 0
+    pattern = re.compile(r"\((float|int|uint)([234])\)\s*\{|\((ModelValue|model_value_t)\)\s*\{")
+    while True:
+        m = pattern.search(text, i)
+        if not m:
+            out.append(text[i:])
+            break
+        out.append(text[i:m.start()])
+        depth, j = 1, m.end()
+        while depth:
+            depth += {"{": 1, "}": -1}.get(text[j], 0)
+            j += 1
+        inner = text[m.end():j - 1]
+        if m.group(1):
+            out.append(f"make_{m.group(1)}{m.group(2)}({inner})")
+        else:
+            out.append(f"{m.group(3)}{{{inner}}}")
+        i = j
+    return "".join(out)
+
+
+def to_cpp(source, kernel_dir, name):
+    text = inline_includes(source, kernel_dir)
+    text = rewrite_literals(text)
+    text = text.replace(str(N_STEPS_SENTINEL), "tgref_n_steps")
+    text = text.replace("orientation = algorithm_update_orientation(",
+                        "++tgref_steps; orientation = algorithm_update_orientation(")
+    # algorithm.py:219 draws two normals inside one expression; C leaves the
+    # order of the two calls unspecified.  clang (pocl, the reference's CI
+    # platform) evaluates them left to right, g++ right to left: sequence them
+    # left to right explicitly so this build draws what the reference draws.
+    text = re.sub(r"noise\s*=\s*randn\(rng_state\)\s*\*\s*et\s*\+\s*randn\(rng_state\)\s*\*\s*ep\s*;",
+                  "{ const float tgref_n1 = randn(rng_state); const float tgref_n2 = randn(rng_state); "
+                  "noise = tgref_n1 * et + tgref_n2 * ep; }", text)
+    return (f'#include "clshim.hpp"\n'
+            f"extern unsigned int tgref_n_steps;\n"
+            f"extern thread_local unsigned long long tgref_steps;\n"
+            f"namespace {name} {{\n{text}\n}}\n")
+
+
+DRIVER = """
+extern "C" unsigned long long tgref_{name}(const int* mask, const unsigned int* mdims, const float* minv,
+        const float* field, const unsigned int* fdims, const float* finv, float step, float gamma, float noise,
+        unsigned int rng_seed, const float* seeds, unsigned int n_seeds, float* out, unsigned int* lengths,
+        float save_at, unsigned int n_steps, int threads)
+{{
+    tgref_n_steps = n_steps;
+    const float4 dummy4 = make_float4(0.0f);
+    const uint4 dummyu4 = make_uint4(0u);
+    const int4 dummyi4 = make_int4(0);
+    const float dummyf = 0.0f;
+    const unsigned int dummyu = 0;
+    unsigned long long total = 0;
+    long g;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : total) num_threads(threads > 0 ? threads : 1)
+    for (g = 0; g < (long)n_seeds; ++g) {{
+        tgref_global_id = (size_t)g;
+        tgref_steps = 0;
+        {name}::tractogram(&dummy4, &dummyu4, &dummyf, 1u, &dummy4, &dummy4, &dummyi4, &dummyu, 1u,
+            mask, make_uint3(mdims[0], mdims[1], mdims[2]), (const float4*)minv,
+            field, make_uint4(fdims[0], fdims[1], fdims[2], fdims[3]), (const float4*)finv,
+            step, gamma{noise_arg}, rng_seed, (const float4*)seeds, n_seeds, (float4*)out, lengths, save_at);
+        total += tgref_steps;
+    }}
+    return total;
+}}
+"""
+
+
+UPDATE_DRIVER = """
+extern "C" void tgref_update_{name}(float step, float gamma, float noise, unsigned int rng_seed,
+        const float* params, const float* orientations, unsigned int n, float* out)
+{{
+    for (unsigned int g = 0; g < n; ++g) {{
+        tgref_global_id = g;
+        {name}::update_orientation(step, gamma{noise_arg}, rng_seed, params, (const float4*)orientations, n,
+                                   (float4*)out);
+    }}
+}}
+"""
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    reference = Path(args.reference)
+    sys.path.insert(0, str(HERE.parent))
+    from oracle.refstubs import install_stubs
+
+    install_stubs(reference)
+    import tractography as ref  # the reference package
+
+    kernel_dir = reference / "tractography" / "resources" / "kernels"
+    OUT.mkdir(exist_ok=True)
+    objects = []
+    common = OUT / "tgref_common.cpp"
+    common.write_text('#include <cstddef>\nthread_local size_t tgref_global_id;\nunsigned int tgref_n_steps;\n'
+                      'thread_local unsigned long long tgref_steps;\n')
+    sources = [common]
+    for name, model, C, algorithm in VARIANTS:
+        src = capture(ref, model, C, algorithm)
+        cpp = to_cpp(src, kernel_dir, name)
+        cpp += DRIVER.format(name=name, noise_arg=", noise" if algorithm == "diffusion" else "")
+        path = OUT / f"tgref_{name}.cpp"
+        path.write_text(cpp)
+        sources.append(path)
+        uname = "u_" + name
+        ucpp = to_cpp(capture_update(ref, model, C, algorithm), kernel_dir, uname)
+        ucpp += UPDATE_DRIVER.format(name=uname, noise_arg=", noise" if algorithm == "diffusion" else "")
+        upath = OUT / f"tgref_{uname}.cpp"
+        upath.write_text(ucpp)
+        sources.append(upath)
+    flags = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-march=x86-64-v3",
+             "-mtune=generic", "-w", f"-I{HERE}"]
+    procs = []
+    for src in sources:
+        obj = src.with_suffix(".o")
+        objects.append(obj)
+        procs.append(subprocess.Popen(["g++", *flags, "-c", str(src), "-o", str(obj)]))
+    if any(p.wait() != 0 for p in procs):
+        raise SystemExit("compiling the reference kernels failed")
+    subprocess.run(["g++", "-shared", "-fopenmp", "-o", str(OUT / "libtgref.so"), *map(str, objects)], check=True)
+    print(f"built {OUT / 'libtgref.so'} ({len(VARIANTS)} kernel variants)")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,91 @@
+"""ctypes access to oracle/_ref/libtgref.so: the reference's kernels run on the CPU.
+
+Test infrastructure only (tests, smoke check, benchmark CPU legs).  The
+library is built by oracle/build_ref.py from the reference sources; it is
+absent where the reference tree is not available, and callers must check
+``available()``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "_ref" / "libtgref.so"
+_lib = None
+
+
+def available() -> bool:
+    return LIB_PATH.exists()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(str(LIB_PATH))
+    return _lib
+
+
+def _variant(model: str, n_coefficients: int, algorithm: str) -> str:
+    if model == "dti":
+        return f"dti_{algorithm}"
+    return f"sh{n_coefficients}_{algorithm}"
+
+
+def tractogram_raw(mask, mask_inv_affine, field, field_inv_affine, model, algorithm, step_size, gamma,
+                   noise_variance, rng_seed, seeds, save_at, n_steps, threads=1):
+    """Run the reference kernel; returns (dense (n, n_steps, 4) points, lengths, accepted steps)."""
+    field = np.ascontiguousarray(field, dtype=np.float32)
+    mask = np.ascontiguousarray(np.asarray(mask) != 0, dtype=np.int32)
+    seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+    minv = np.ascontiguousarray(mask_inv_affine, dtype=np.float32)
+    finv = np.ascontiguousarray(field_inv_affine, dtype=np.float32)
+    mdims = np.array(mask.shape, dtype=np.uint32)
+    fdims = np.array(field.shape, dtype=np.uint32)
+    n = len(seeds)
+    out = np.zeros((n, n_steps, 4), np.float32)
+    lengths = np.zeros(n, np.uint32)
+    fn = getattr(lib(), "tgref_" + _variant(model, field.shape[3], algorithm))
+    fn.restype = ctypes.c_ulonglong
+    P = ctypes.c_void_p
+    fn.argtypes = [P, P, P, P, P, P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_uint, P,
+                   ctypes.c_uint, P, P, ctypes.c_float, ctypes.c_uint, ctypes.c_int]
+    steps = fn(mask.ctypes.data, mdims.ctypes.data, minv.ctypes.data, field.ctypes.data, fdims.ctypes.data,
+               finv.ctypes.data, step_size, gamma, noise_variance, rng_seed & 0xFFFFFFFF, seeds.ctypes.data, n,
+               out.ctypes.data, lengths.ctypes.data, save_at, n_steps, threads)
+    return out, lengths, int(steps)
+
+
+def tractogram(domain, field, algorithm, seeds, rng_seed, save_at, n_steps, threads=1):
+    """Same as tractogram_raw for package domain/field/algorithm objects."""
+    model = "dti" if algorithm.local_model.n_parameters == 6 and type(algorithm.local_model).__name__ == \
+        "DiffusionTensorImaging" else "sh"
+    kind = "diffusion" if hasattr(algorithm, "noise_variance") else "transport"
+    return tractogram_raw(domain.values, domain.inverse_affine, field.values, field.inverse_affine, model, kind,
+                          algorithm.step_size, algorithm.gamma, getattr(algorithm, "noise_variance", 0.0),
+                          rng_seed, seeds, save_at, n_steps, threads)
+
+
+def tractogram_steps(domain, field, kind, step_size, gamma, noise_variance, seeds, rng_seed, save_at, n_steps,
+                     threads):
+    """Accepted steps of a reference-kernel run (for timing)."""
+    model = "sh" if field.values.shape[3] != 6 else "dti"
+    return tractogram_raw(domain.values, domain.inverse_affine, field.values, field.inverse_affine, model, kind,
+                          step_size, gamma, noise_variance, rng_seed, seeds, save_at, n_steps, threads)[2]
+
+
+def update_orientation(model, n_coefficients, algorithm, step_size, gamma, noise_variance, rng_seed, params,
+                       orientations):
+    """The reference's standalone orientation-update kernel, one row per orientation."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    o4 = np.zeros((len(orientations), 4), np.float32)
+    o4[:, :3] = orientations
+    out = np.zeros_like(o4)
+    fn = getattr(lib(), "tgref_update_u_" + _variant(model, n_coefficients, algorithm))
+    P = ctypes.c_void_p
+    fn.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_uint, P, P, ctypes.c_uint, P]
+    fn(step_size, gamma, noise_variance, rng_seed & 0xFFFFFFFF, params.ctypes.data, o4.ctypes.data, len(o4),
+       out.ctypes.data)
+    return out[:, :3]

@@ -1,0 +1,116 @@
+"""The oracle against the reference's own kernels compiled for the CPU (oracle/_ref).
+
+oracle/build_ref.py builds libtgref.so from the OpenCL source the reference
+assembles itself (build() runs it where the reference tree is present).
+These tests pin the oracle -- and through the bit-exact GPU tests, the CUDA
+path -- to the reference kernel:
+
+* known answers of the reference's tests on the reference kernel;
+* Diffusion with the reference's MWC64X noise stream: point-wise within
+  1e-4 voxel over the first 100 steps for >= 99.9 % of seeds, identical
+  lengths;
+* non-chaotic Transport cases (exact u0u3 solution, circle): point-wise;
+* chaotic config-0 Transport (step 0.1 voxel): single-step float32 error of
+  the oracle against the reference's float64 NumPy update no larger than the
+  reference kernel's own, and the length distributions of the two agree
+  (two-sample KS test).
+"""
+
+import numpy as np
+import pytest
+
+import tractography_b200 as tg
+from oracle import oracle as O
+from oracle import reference as R
+from tractography_b200 import synthetic
+
+import data
+from helpers import oracle_case
+
+pytestmark = pytest.mark.skipif(not R.available(), reason="oracle/_ref not built (reference sources absent)")
+
+
+def test_reference_kernel_known_answers():
+    """test/test_tracking.py:28-100 on the reference kernel itself."""
+    f = np.zeros((1, 1, 1, 15), np.float32)
+    f[..., 0] = 1.0
+    s = np.array([[0, 0, 0, 1, 1, 0, 0, 0]], np.float32)
+    out, n, _ = R.tractogram_raw(np.ones((1, 1, 1)), np.eye(4), f, np.eye(4), "sh", "transport", 1.0, 0.0, 0.0, 0,
+                                 s, 1.0, 300)
+    np.testing.assert_allclose(out[0, : n[0], :3], [[0, 0, 0], [1, 0, 0]], atol=1e-6)
+    f = np.zeros((20, 1, 1, 15), np.float32)
+    f[..., 0] = 1.0
+    out, n, _ = R.tractogram_raw(np.ones((20, 1, 1)), np.eye(4), f, np.eye(4), "sh", "transport", 0.25, 0.0, 0.0,
+                                 0, s, 0.5, 6)
+    np.testing.assert_allclose(out[0, :6, 0], np.arange(0.0, 3.0, 0.5), atol=1e-6)
+
+
+def test_diffusion_first_100_steps_match_reference_kernel():
+    fod, mask = synthetic.bundle_field((48, 56, 48), lmax=8, seed=3, voxel_mm=1.25)
+    field = tg.field.Image(fod)
+    domain = tg.domain.Image(tg.Nifti1Image(np.any(field.values != 0, -1).astype(np.uint8), fod.affine))
+    seeds = synthetic.uniform_seeds(mask, 4000, seed=1)
+    alg = tg.algorithm.Diffusion(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.001, gamma=1.0,
+                                 noise_variance=0.1, seed=0)
+    ref, ref_len, _ = R.tractogram(domain, field, alg, seeds, 12345, 0.001, 101, threads=8)
+    got, got_len = oracle_case(alg, domain, field, rng_seed=12345, save_at=0.001, n_steps=101).tractogram(
+        seeds, n_threads=8)
+    assert np.array_equal(ref_len, got_len)
+    deviation = np.abs(ref[:, :, :3] - got[:, :, :3]).max(axis=(1, 2)) / 1.25      # voxels
+    assert np.mean(deviation <= 1e-4) >= 0.999
+
+
+@pytest.mark.parametrize("algorithm", ["transport", "diffusion"])
+def test_u0u3_matches_reference_kernel(algorithm):
+    coef = data.u0u3_coefficients(0.3, 45)
+    f = np.broadcast_to(coef, (1, 1, 1, 45)).astype(np.float32).copy()
+    A = np.diag((1000.0, 1000.0, 1000.0, 1.0))
+    A[:3, 3] = -0.5
+    inv = np.linalg.inv(A).astype(np.float32)
+    o = np.asarray(tg.core.sph2cart(0.5, 0.12, 1.0))
+    s = np.array([[10, 10, 10, 1, *o, 0]], np.float32)
+    ref, ref_len, _ = R.tractogram_raw(np.ones((1, 1, 1)), inv, f, inv, "sh", algorithm, 0.001, 1.0, 0.0, 5, s,
+                                       0.001, 1000)
+    case = O.Case(mask=np.ones((1, 1, 1)), mask_inv_affine=inv, field=f, field_inv_affine=inv,
+                  algorithm=O.ALGO_TRANSPORT if algorithm == "transport" else O.ALGO_DIFFUSION, step_size=0.001,
+                  gamma=1.0, noise_variance=0.0, rng_seed=5, save_at=0.001, n_steps=1000)
+    got, got_len = case.tractogram(s)
+    assert np.array_equal(ref_len, got_len)
+    np.testing.assert_allclose(got[0, : got_len[0], :3], ref[0, : ref_len[0], :3], atol=1e-4)
+
+
+def test_circle_matches_reference_kernel():
+    fod = data.circle(shape=(10, 10, 1), radius=2).astype(np.float32)
+    wm = fod[..., 0] > 0
+    s = np.array([[4.5, 6.5, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0]], np.float32)
+    ref, ref_len, _ = R.tractogram_raw(wm, np.eye(4), fod, np.eye(4), "sh", "transport", 1e-4, 50.0, 0.0, 0, s,
+                                       0.25, 400)
+    got, got_len = O.Case(mask=wm, mask_inv_affine=np.eye(4), field=fod, field_inv_affine=np.eye(4),
+                          step_size=1e-4, gamma=50.0, save_at=0.25, n_steps=400).tractogram(s)
+    assert ref_len[0] == got_len[0] == 400
+    np.testing.assert_allclose(got[0, :400, :3], ref[0, :400, :3], atol=1e-4)
+
+
+def test_config0_transport_single_step_and_length_distribution():
+    from scipy.stats import ks_2samp
+
+    fod, mask = synthetic.config0()
+    field = tg.field.Image(fod)
+    domain = tg.domain.Image(mask)
+    seeds = synthetic.seeds_in_mask(mask, 2000, seed=0)
+    params = field.evaluate(seeds[:, :3])
+    o = seeds[:, 4:7]
+    alg = tg.algorithm.Transport(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.2, gamma=1.0)
+    exact = alg.update_orientation(params.astype(np.float64), o.astype(np.float64))
+    ref1 = R.update_orientation("sh", 45, "transport", 0.2, 1.0, 0.0, 0, params, o)
+    got1 = O.Case(algorithm=O.ALGO_TRANSPORT, step_size=0.2, gamma=1.0).update_orientation(params, o)
+    err_ref = np.median(np.abs(ref1 - exact).max(axis=1))
+    err_got = np.median(np.abs(got1 - exact).max(axis=1))
+    assert err_got <= 1.2 * err_ref
+    ref, ref_len, _ = R.tractogram(domain, field, alg, seeds, 0, 0.25, 1200, threads=8)
+    got, got_len = oracle_case(alg, domain, field, save_at=0.25, n_steps=1200).tractogram(seeds, n_threads=8)
+    assert ks_2samp(ref_len, got_len).pvalue > 0.01
+    ends_ref = ref[np.arange(len(seeds)), ref_len - 1, :3]
+    ends_got = got[np.arange(len(seeds)), got_len - 1, :3]
+    for axis in range(3):
+        assert ks_2samp(ends_ref[:, axis], ends_got[:, axis]).pvalue > 0.01

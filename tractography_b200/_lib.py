@@ -41,6 +41,7 @@ EXPORTS = (
     "tg_tracker_create",
     "tg_tracker_destroy",
     "tg_tracker_run",
+    "tg_tracker_run_jobs",
     "tg_tracker_stats",
     "tg_tracker_copy_points",
     "tg_seeds_from_fod",
@@ -64,6 +65,22 @@ class Algorithm(ctypes.Structure):
         ("rng_seed", ctypes.c_uint32),
         ("philox_key", ctypes.c_uint64),
         ("seed_offset", ctypes.c_uint64),
+    ]
+
+
+class Job(ctypes.Structure):
+    """Mirror of ``tg_job``."""
+
+    _fields_ = [
+        ("domain", ctypes.c_void_p),
+        ("field", ctypes.c_void_p),
+        ("algorithm", Algorithm),
+        ("seeds", ctypes.c_void_p),
+        ("n_seeds", ctypes.c_uint32),
+        ("batch_size", ctypes.c_uint32),
+        ("batch_rng_seeds", ctypes.c_void_p),
+        ("save_at", ctypes.c_float),
+        ("n_steps", ctypes.c_uint32),
     ]
 
 
@@ -108,6 +125,8 @@ def load() -> ctypes.CDLL:
         "tg_tracker_destroy": ([P], ctypes.c_int),
         "tg_tracker_run": ([P, AP, P, P, P, ctypes.c_int, U32, U32, P, F, U32, P, P,
                             ctypes.POINTER(U64), ctypes.POINTER(U64), P], ctypes.c_int),
+        "tg_tracker_run_jobs": ([P, ctypes.POINTER(Job), U32, ctypes.c_int, P, P, ctypes.POINTER(U64),
+                                 ctypes.POINTER(U64), P], ctypes.c_int),
         "tg_tracker_stats": ([P, ctypes.POINTER(F), ctypes.POINTER(U32), ctypes.POINTER(U32)], ctypes.c_int),
         "tg_tracker_copy_points": ([P, P, U64, U64, ctypes.c_int, P], ctypes.c_int),
         "tg_seeds_from_fod": ([I32, U32, P, P, U32, P, P, U32, P, P], ctypes.c_int),

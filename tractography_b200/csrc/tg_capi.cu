@@ -51,6 +51,17 @@ struct tg_tracker {
     std::vector<uint32_t> h_len;
     std::vector<uint32_t> h_done;
     std::vector<uint32_t> h_retry;
+    // multi-job runs: one stream per code path, job and class tables
+    cudaStream_t class_stream[kClassKinds] = {};
+    cudaEvent_t class_done[kClassKinds] = {};
+    cudaEvent_t ev_fork = nullptr;
+    JobDev* d_jobs = nullptr;
+    size_t cap_jobs = 0;
+    uint32_t* d_job_base = nullptr;
+    size_t cap_job_base = 0;
+    uint32_t* d_class_lists = nullptr;   // job lists and prefixes of all classes
+    size_t cap_class_lists = 0;
+    unsigned long long* d_class_counters = nullptr;
     // statistics of the last run
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     float kernel_ms = 0.0f;
@@ -371,6 +382,15 @@ int tg_tracker_destroy(tg_tracker* t)
     cudaFree(t->points);
     if (t->ev_start) cudaEventDestroy(t->ev_start);
     if (t->ev_stop) cudaEventDestroy(t->ev_stop);
+    for (int k = 0; k < kClassKinds; ++k) {
+        if (t->class_stream[k]) cudaStreamDestroy(t->class_stream[k]);
+        if (t->class_done[k]) cudaEventDestroy(t->class_done[k]);
+    }
+    if (t->ev_fork) cudaEventDestroy(t->ev_fork);
+    cudaFree(t->d_jobs);
+    cudaFree(t->d_job_base);
+    cudaFree(t->d_class_lists);
+    cudaFree(t->d_class_counters);
     delete t;
     return TG_OK;
 }
@@ -568,6 +588,261 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
         t->launches += 1;
         t->total_points = total;
         wave_items.assign(t->h_retry.begin(), t->h_retry.end());
+        first_wave = false;
+    }
+    unsigned long long steps = 0;
+    TG_TRY(cudaMemcpyAsync(&steps, t->counters + 1, sizeof steps, cudaMemcpyDeviceToHost, s));
+    TG_TRY(cudaStreamSynchronize(s));
+    t->total_points = total;
+    if (total_points) *total_points = total;
+    if (total_steps) *total_steps = steps;
+    return TG_OK;
+}
+
+int tg_tracker_run_jobs(tg_tracker* t, const tg_job* jobs, uint32_t n_jobs, int seeds_on_host, uint32_t* h_lengths,
+                        uint64_t* h_offsets, uint64_t* total_points, uint64_t* total_steps, void* stream)
+{
+    if (t == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "tracker is null");
+    t->total_points = 0;
+    t->kernel_ms = 0.0f;
+    t->waves = 0;
+    t->launches = 0;
+    if (total_points) *total_points = 0;
+    if (total_steps) *total_steps = 0;
+    if (n_jobs == 0) return TG_OK;
+    if (jobs == nullptr || h_lengths == nullptr || h_offsets == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null buffer");
+    cudaStream_t s = as_stream(stream);
+
+    // Validate the jobs and lay them out in one global seed index space.
+    std::vector<JobDev> table(n_jobs);
+    std::vector<uint32_t> job_base(n_jobs + 1, 0);
+    std::vector<uint32_t> rng_base(n_jobs, 0);
+    std::vector<int> kind(n_jobs, 0);
+    uint64_t n_total = 0, n_batches_total = 0, worst = 0;
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+        const tg_job& J = jobs[j];
+        TrackParams tp;
+        int st = make_track_params(&J.algorithm, J.domain, J.field, J.save_at, J.n_steps, &tp);
+        if (st != TG_OK) return fail(st, "job " + std::to_string(j) + ": " + g_error);
+        if (J.n_steps == 0) return fail(TG_ERR_INVALID_ARGUMENT, "job " + std::to_string(j) + ": n_steps must be positive");
+        if (J.n_seeds > 0 && (J.seeds == nullptr || J.batch_rng_seeds == nullptr || J.batch_size == 0))
+            return fail(TG_ERR_INVALID_ARGUMENT, "job " + std::to_string(j) + ": missing seeds or batch seeds");
+        std::memset(&table[j], 0, sizeof(JobDev));
+        table[j].t = tp;
+        table[j].n_seeds = J.n_seeds;
+        table[j].batch_size = J.batch_size > 0 ? J.batch_size : 1;
+        table[j].seed_offset = J.algorithm.seed_offset;
+        kind[j] = class_kind(J.field->d.model, J.field->d.lmax, J.algorithm.algorithm);
+        job_base[j] = (uint32_t)n_total;
+        rng_base[j] = (uint32_t)n_batches_total;
+        n_total += J.n_seeds;
+        n_batches_total += (J.n_seeds + table[j].batch_size - 1) / table[j].batch_size;
+        worst += (uint64_t)J.n_seeds * (((uint64_t)J.n_steps + kChunkPoints - 1) / kChunkPoints * kChunkPoints);
+        if (n_total >= 0x80000000ull) return fail(TG_ERR_INVALID_ARGUMENT, "too many seeds in one run");
+    }
+    job_base[n_jobs] = (uint32_t)n_total;
+    if (n_total == 0) return TG_OK;
+
+    // Device copies: seeds (when given on the host), batch seeds, tables.
+    TG_TRY(ensure(&t->batch_seeds, &t->cap_batches, n_batches_total));
+    TG_TRY(ensure(&t->seeds, &t->cap_seed_copy, seeds_on_host ? (size_t)n_total * 2 : 1));
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+        const tg_job& J = jobs[j];
+        if (J.n_seeds == 0) continue;
+        const uint64_t nb = (J.n_seeds + table[j].batch_size - 1) / table[j].batch_size;
+        TG_TRY(cudaMemcpyAsync(t->batch_seeds + rng_base[j], J.batch_rng_seeds, nb * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, s));
+        if (seeds_on_host) {
+            TG_TRY(cudaMemcpyAsync(t->seeds + 2 * (size_t)job_base[j], J.seeds, (size_t)J.n_seeds * 8 * sizeof(float),
+                                   cudaMemcpyHostToDevice, s));
+            table[j].seeds = t->seeds + 2 * (size_t)job_base[j];
+        } else {
+            table[j].seeds = reinterpret_cast<const float4*>(J.seeds);
+        }
+        table[j].rng_base = rng_base[j];
+    }
+    TG_TRY(ensure(&t->d_jobs, &t->cap_jobs, n_jobs));
+    TG_TRY(ensure(&t->d_job_base, &t->cap_job_base, n_jobs + 1));
+    TG_TRY(cudaMemcpyAsync(t->d_jobs, table.data(), n_jobs * sizeof(JobDev), cudaMemcpyHostToDevice, s));
+    TG_TRY(cudaMemcpyAsync(t->d_job_base, job_base.data(), (n_jobs + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+
+    // Classes: jobs grouped by code path, longest point budget first.
+    std::vector<std::vector<uint32_t>> members(kClassKinds);
+    for (uint32_t j = 0; j < n_jobs; ++j)
+        if (jobs[j].n_seeds > 0) members[kind[j]].push_back(j);
+    std::vector<uint32_t> lists;            // per class: jobs then prefix (n + 1)
+    std::vector<size_t> list_at(kClassKinds, 0);
+    for (int k = 0; k < kClassKinds; ++k) {
+        auto& m = members[k];
+        std::stable_sort(m.begin(), m.end(), [&](uint32_t a, uint32_t b) { return jobs[a].n_steps > jobs[b].n_steps; });
+        list_at[k] = lists.size();
+        lists.insert(lists.end(), m.begin(), m.end());
+        uint32_t acc = 0;
+        lists.push_back(0);
+        for (uint32_t j : m) {
+            acc += jobs[j].n_seeds;
+            lists.push_back(acc);
+        }
+    }
+    TG_TRY(ensure(&t->d_class_lists, &t->cap_class_lists, lists.size()));
+    TG_TRY(cudaMemcpyAsync(t->d_class_lists, lists.data(), lists.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    if (t->d_class_counters == nullptr)
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->d_class_counters), kClassKinds * sizeof(unsigned long long)));
+    if (t->ev_fork == nullptr) TG_TRY(cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming));
+    for (int k = 0; k < kClassKinds; ++k) {
+        if (members[k].empty() || t->class_stream[k] != nullptr) continue;
+        TG_TRY(cudaStreamCreateWithFlags(&t->class_stream[k], cudaStreamNonBlocking));
+        TG_TRY(cudaEventCreateWithFlags(&t->class_done[k], cudaEventDisableTiming));
+    }
+
+    // Per-seed buffers and the point pool.
+    if (t->cap_seeds < n_total) {
+        cudaFree(t->first_chunk);
+        cudaFree(t->lengths);
+        cudaFree(t->offsets);
+        cudaFree(t->ids);
+        cudaFree(t->done_ids);
+        t->first_chunk = nullptr;
+        t->lengths = nullptr;
+        t->offsets = nullptr;
+        t->ids = nullptr;
+        t->done_ids = nullptr;
+        t->cap_seeds = 0;
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->first_chunk), n_total * sizeof(int32_t)));
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->lengths), n_total * sizeof(uint32_t)));
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->offsets), n_total * sizeof(uint64_t)));
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->ids), n_total * sizeof(uint32_t)));
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->done_ids), n_total * sizeof(uint32_t)));
+        t->cap_seeds = n_total;
+    }
+    uint64_t want = t->pool_points_request;
+    if (want == 0) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const uint64_t budget = (uint64_t)(free_b / 3) / (3 * sizeof(float) + 1);
+        want = std::min<uint64_t>(worst, std::max<uint64_t>(budget, (uint64_t)1 << 20));
+    }
+    int st = tracker_pool(t, want);
+    if (st != TG_OK) return st;
+
+    MultiParams mp;
+    std::memset(&mp, 0, sizeof mp);
+    mp.jobs = t->d_jobs;
+    mp.job_base = t->d_job_base;
+    mp.n_jobs = n_jobs;
+    mp.batch_rng_seeds = t->batch_seeds;
+    mp.chunk_counter = t->chunk_counter;
+    mp.first_chunk = t->first_chunk;
+    mp.lengths = t->lengths;
+    mp.steps_done = t->counters + 1;
+    const int sms = sm_count();
+
+    t->h_len.resize(n_total);
+    TG_TRY(cudaMemsetAsync(t->counters + 1, 0, sizeof(unsigned long long), s));
+    uint64_t total = 0;
+    bool first_wave = true;
+    int stalls = 0;
+    std::vector<std::vector<uint32_t>> retry(kClassKinds);
+    std::vector<uint32_t> wave_ids;
+    while (true) {
+        // per class: its item source for this wave
+        std::vector<size_t> retry_at(kClassKinds, 0);
+        uint64_t wave_items = 0;
+        wave_ids.clear();
+        for (int k = 0; k < kClassKinds; ++k) {
+            retry_at[k] = wave_ids.size();
+            if (!first_wave) wave_ids.insert(wave_ids.end(), retry[k].begin(), retry[k].end());
+        }
+        if (!first_wave) {
+            if (wave_ids.empty()) break;
+            TG_TRY(cudaMemcpyAsync(t->ids, wave_ids.data(), wave_ids.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        }
+        mp.pool = t->pool;
+        mp.chunk_next = t->chunk_next;
+        mp.n_chunks = t->n_chunks;
+        TG_TRY(cudaMemsetAsync(t->d_class_counters, 0, kClassKinds * sizeof(unsigned long long), s));
+        TG_TRY(cudaMemsetAsync(t->chunk_counter, 0, sizeof(unsigned int), s));
+        TG_TRY(cudaEventRecord(t->ev_start, s));
+        TG_TRY(cudaEventRecord(t->ev_fork, s));
+        std::vector<int> launched;
+        // classes with the most point budget first
+        std::vector<int> order;
+        for (int k = 0; k < kClassKinds; ++k) order.push_back(k);
+        std::vector<uint64_t> budget(kClassKinds, 0);
+        for (int k = 0; k < kClassKinds; ++k)
+            for (uint32_t j : members[k]) budget[k] += (uint64_t)jobs[j].n_seeds * jobs[j].n_steps;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return budget[a] > budget[b]; });
+        for (int k : order) {
+            ClassDev cls;
+            std::memset(&cls, 0, sizeof cls);
+            cls.kind = k;
+            cls.n_jobs = (uint32_t)members[k].size();
+            cls.jobs = t->d_class_lists + list_at[k];
+            cls.prefix = t->d_class_lists + list_at[k] + members[k].size();
+            cls.counter = t->d_class_counters + k;
+            if (first_wave) {
+                cls.n_items = members[k].empty() ? 0 : lists[list_at[k] + 2 * members[k].size()];
+            } else {
+                cls.item_ids = t->ids + retry_at[k];
+                cls.n_items = (uint32_t)retry[k].size();
+            }
+            if (cls.n_items == 0) continue;
+            wave_items += cls.n_items;
+            TG_TRY(cudaStreamWaitEvent(t->class_stream[k], t->ev_fork, 0));
+            TG_TRY(launch_track_class(mp, cls, sms, t->class_stream[k]));
+            TG_TRY(cudaEventRecord(t->class_done[k], t->class_stream[k]));
+            TG_TRY(cudaStreamWaitEvent(s, t->class_done[k], 0));
+            launched.push_back(k);
+            t->launches += 1;
+        }
+        TG_TRY(cudaEventRecord(t->ev_stop, s));
+        TG_TRY(cudaMemcpyAsync(t->h_len.data(), t->lengths, n_total * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        TG_TRY(cudaStreamSynchronize(s));
+        float wave_ms = 0.0f;
+        TG_TRY(cudaEventElapsedTime(&wave_ms, t->ev_start, t->ev_stop));
+        t->kernel_ms += wave_ms;
+        t->waves += 1;
+
+        // collect finished streamlines, queue the others for the next wave
+        t->h_done.clear();
+        std::vector<std::vector<uint32_t>> next(kClassKinds);
+        auto visit = [&](uint32_t g, int k) {
+            const uint32_t L = t->h_len[g];
+            if (L & kOverflowBit) {
+                next[k].push_back(g);
+            } else {
+                t->h_done.push_back(g);
+                h_offsets[g] = total;
+                h_lengths[g] = L;
+                total += L;
+            }
+        };
+        for (int k : launched) {
+            if (first_wave) {
+                for (uint32_t j : members[k])
+                    for (uint32_t i = 0; i < jobs[j].n_seeds; ++i) visit(job_base[j] + i, k);
+            } else {
+                for (uint32_t g : retry[k]) visit(g, k);
+            }
+        }
+        (void)wave_items;
+        if (t->h_done.empty()) {
+            if (++stalls > 4) return fail(TG_ERR_POOL_EXHAUSTED, "point pool too small for one streamline");
+            st = tracker_pool(t, (uint64_t)t->n_chunks * kChunkPoints * 4);
+            if (st != TG_OK) return st;
+        } else {
+            st = tracker_points(t, total, s);
+            if (st != TG_OK) return st;
+            TG_TRY(cudaMemcpyAsync(t->offsets, h_offsets, n_total * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+            TG_TRY(cudaMemcpyAsync(t->done_ids, t->h_done.data(), t->h_done.size() * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, s));
+            TG_TRY(launch_gather(t->pool, t->chunk_next, t->first_chunk, t->lengths, t->offsets, t->done_ids,
+                                 (uint32_t)t->h_done.size(), t->points, s));
+            t->launches += 1;
+            t->total_points = total;
+        }
+        retry.swap(next);
         first_wave = false;
     }
     unsigned long long steps = 0;

@@ -81,8 +81,14 @@ TGM_FN float tgm_pow2i(int k)
 /* Quadrant index from the rounded reduction multiple (NaN/huge -> 0). */
 TGM_FN int tgm_quadrant(float q)
 {
-    return (q == q && fabsf(q) < 8388608.0f) ? (int)q : 0;
+    const float finite_q = (q == q && fabsf(q) < 8388608.0f) ? q : 0.0f;
+    return (int)finite_q;
 }
+
+/* The functions below compute their main path for every input and patch
+ * special inputs (NaN, infinities, out-of-range) with selects at the end, so
+ * GPU warps do not branch on data; the values are those of the obvious
+ * early-return formulation. */
 
 /*
  * sincos: s = sin(x), c = cos(x).  Reduction x = q*pi/2 + r, |r| <~ pi/4.
@@ -110,14 +116,12 @@ TGM_FN void tgm_sincosf(float x, float* s_out, float* c_out)
     pc = fmaf(pc, r2, -0.5f);
     const float cr = fmaf(r2, pc, 1.0f);
 
+    /* quadrant 0: (sr, cr); 1: (cr, -sr); 2: (-sr, -cr); 3: (-cr, sr) */
     const int quadrant = tgm_quadrant(q) & 3;
-    float s, c;
-    if (quadrant == 0) { s = sr;  c = cr;  }
-    else if (quadrant == 1) { s = cr;  c = -sr; }
-    else if (quadrant == 2) { s = -sr; c = -cr; }
-    else { s = -cr; c = sr;  }
-    *s_out = s;
-    *c_out = c;
+    const float s = (quadrant & 1) ? cr : sr;
+    const float c = (quadrant & 1) ? sr : cr;
+    *s_out = (quadrant & 2) ? -s : s;
+    *c_out = ((quadrant + 1) & 2) ? -c : c;
 }
 
 TGM_FN float tgm_cosf(float x)
@@ -137,11 +141,10 @@ TGM_FN float tgm_sinf(float x)
 /*
  * exp: x = k ln2 + r, |r| <= ln2/2; e^r by Taylor to r^7; scale by 2^k.
  */
-TGM_FN float tgm_expf(float x)
+TGM_FN float tgm_expf(float x_in)
 {
-    if (x != x) return x;
-    if (x > 88.72284f) return tgm_u2f(0x7f800000u);   /* +inf */
-    if (x < -103.97208f) return 0.0f;
+    /* main path on the input clamped to the finite-result range */
+    const float x = fminf(fmaxf(x_in, -103.97208f), 88.72284f);
     const float k = rintf(x * TGM_LOG2E);
     float r = fmaf(-k, TGM_LN2_HI, x);
     r = fmaf(-k, TGM_LN2_LO, r);
@@ -153,26 +156,23 @@ TGM_FN float tgm_expf(float x)
     p = fmaf(p, r, 0.5f);
     p = fmaf(p, r, 1.0f);
     p = fmaf(p, r, 1.0f);
-    const int ki = (int)k;                       /* |k| <= 150 here */
+    const int ki = (int)k;                       /* -150 <= k <= 128 here */
     const int k1 = ki / 2;
     const int k2 = ki - k1;
-    return (p * tgm_pow2i(k1)) * tgm_pow2i(k2);
+    float result = (p * tgm_pow2i(k1)) * tgm_pow2i(k2);
+    result = (x_in > 88.72284f) ? tgm_u2f(0x7f800000u) : result;   /* +inf */
+    result = (x_in < -103.97208f) ? 0.0f : result;
+    return (x_in != x_in) ? x_in : result;
 }
 
 /*
  * log: natural logarithm for binary32.
  */
-TGM_FN float tgm_logf(float x)
+TGM_FN float tgm_logf(float x_in)
 {
-    if (x != x) return x;
-    if (x < 0.0f) return tgm_u2f(0x7fc00000u);        /* NaN */
-    if (x == 0.0f) return tgm_u2f(0xff800000u);       /* -inf */
-    if (x == tgm_u2f(0x7f800000u)) return x;          /* +inf */
-    int e_adjust = 0;
-    if (x < 0x1p-126f) {                              /* subnormal input */
-        x = x * 0x1p+24f;
-        e_adjust = -24;
-    }
+    const int subnormal = x_in < 0x1p-126f;           /* scale subnormals up by 2^24 */
+    const float x = subnormal ? x_in * 0x1p+24f : x_in;
+    const int e_adjust = subnormal ? -24 : 0;
     const uint32_t bits = tgm_f2u(x);
     int e = (int)((bits >> 23) & 0xffu) - 127 + e_adjust;
     float m = tgm_u2f((bits & 0x007fffffu) | 0x3f800000u);   /* [1, 2) */
@@ -191,7 +191,11 @@ TGM_FN float tgm_logf(float x)
     const float two_s = s + s;
     const float logm = fmaf(two_s * z, p, two_s);
     const float ef = (float)e;
-    return fmaf(ef, TGM_LN2_HI, fmaf(ef, TGM_LN2_LO, logm));
+    float result = fmaf(ef, TGM_LN2_HI, fmaf(ef, TGM_LN2_LO, logm));
+    result = (x_in == tgm_u2f(0x7f800000u)) ? x_in : result;          /* +inf */
+    result = (x_in == 0.0f) ? tgm_u2f(0xff800000u) : result;          /* -inf */
+    result = (x_in < 0.0f) ? tgm_u2f(0x7fc00000u) : result;           /* NaN */
+    return (x_in != x_in) ? x_in : result;
 }
 
 #endif /* TG_FMATH_H */

@@ -77,6 +77,54 @@ struct PersistentParams {
     unsigned long long* steps_done;   // total accepted steps
 };
 
+// Many jobs queued at once (tg_multi.cu).  Job j covers global seed indices
+// [job_base[j], job_base[j + 1]); its seeds, field, domain and parameters
+// are in jobs[j].  Jobs are grouped in classes of identical code path
+// (model, lmax, algorithm), each drained by one persistent launch whose
+// lanes refill from the class's queue as their streamlines terminate.
+struct JobDev {
+    TrackParams t;
+    const float4* seeds;
+    uint32_t n_seeds;
+    uint32_t batch_size;
+    uint32_t rng_base;          // index of this job's batch 0 in batch_rng_seeds
+    uint32_t pad;
+    uint64_t seed_offset;       // Philox index base
+};
+
+enum ClassKind : int {
+    kSH0T, kSH0D, kSH2T, kSH2D, kSH4T, kSH4D, kSH6T, kSH6D, kSH8T, kSH8D, kDTIT, kDTID, kClassKinds
+};
+
+struct ClassDev {
+    int kind;
+    uint32_t n_jobs;
+    const uint32_t* jobs;       // job indices of this class, in queue order
+    const uint32_t* prefix;     // n_jobs + 1 prefix sums of their seed counts
+    const uint32_t* item_ids;   // nullable: global seed indices to retry
+    uint32_t n_items;
+    unsigned long long* counter;
+};
+
+struct MultiParams {
+    const JobDev* jobs;
+    const uint32_t* job_base;   // n_jobs + 1
+    uint32_t n_jobs;
+    const uint32_t* batch_rng_seeds;
+    float* pool;
+    int32_t* chunk_next;
+    uint32_t n_chunks;
+    unsigned int* chunk_counter;
+    int32_t* first_chunk;       // per global seed
+    uint32_t* lengths;          // per global seed; kOverflowBit when retried
+    unsigned long long* steps_done;
+};
+
+// One persistent launch per class (code path); classes run concurrently on
+// separate streams and share the point pool.
+cudaError_t launch_track_class(const MultiParams& mp, const ClassDev& cls, int sms, cudaStream_t stream);
+int class_kind(int model, int lmax, int algorithm);
+
 // Launchers (tg_track.cu).
 cudaError_t launch_track_dense(const FieldDev& f, const TrackParams& p, const float4* seeds,
                                uint32_t n_seeds, uint32_t rng_seed, uint64_t seed_offset,

@@ -1,0 +1,184 @@
+/*
+ * tg_multi.cu -- many tracking jobs in one persistent launch.
+ *
+ * A job is one reference `tracking.tractogram` call (its own field, domain,
+ * algorithm parameters, seeds and RNG seeds).  All jobs of a request mix are
+ * queued at once: each class of jobs with the same compiled code path
+ * (model, lmax, algorithm) has a device queue of seeds drained by its own
+ * persistent launch, all classes launched together on concurrent streams;
+ * lanes pull seeds from their class queue and refill as their streamlines
+ * terminate.  Lanes of a warp never diverge across code paths, small
+ * jobs share the GPU with large ones, and no job waits for another job's
+ * longest streamline.  Per-lane job parameters are read from the job table
+ * when a lane takes a new seed.  Output goes to the tracker's chunk pool
+ * exactly as the single-job persistent kernel's does.
+ */
+#include <cuda_runtime.h>
+
+#include "tg_step.cuh"
+
+namespace tg {
+
+int class_kind(int model, int lmax, int algorithm)
+{
+    if (model == kModelDTI) return algorithm == kTransport ? kDTIT : kDTID;
+    const int base = (lmax / 2) * 2;   // kSH0T, kSH2T, ... are consecutive pairs
+    return base + (algorithm == kTransport ? 0 : 1);
+}
+
+namespace {
+
+__device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t* a, uint32_t n, uint32_t v)
+{
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] <= v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ bool m_chunk_alloc(const MultiParams& mp, int32_t& chunk)
+{
+    const unsigned int nc = atomicAdd(mp.chunk_counter, 1u);
+    if (nc >= mp.n_chunks) return false;
+    mp.chunk_next[nc] = -1;
+    chunk = (int32_t)nc;
+    return true;
+}
+
+__device__ __forceinline__ bool m_emit(const MultiParams& mp, int32_t& chunk, uint32_t& fill, float x, float y,
+                                       float z)
+{
+    if (fill == (uint32_t)kChunkPoints) {
+        int32_t nc;
+        if (!m_chunk_alloc(mp, nc)) return false;
+        mp.chunk_next[chunk] = nc;
+        chunk = nc;
+        fill = 0;
+    }
+    float* q = mp.pool + ((size_t)chunk * kChunkPoints + fill) * 3;
+    q[0] = x;
+    q[1] = y;
+    q[2] = z;
+    fill++;
+    return true;
+}
+
+// Drain one class: lanes take seeds from the class queue until it is empty.
+template <int MODEL, int LMAX, int ALGO>
+__device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp, const ClassDev& cls)
+{
+    constexpr int CPAD = ModelShape<MODEL, LMAX>::CPAD;
+    float c[CPAD];
+#pragma unroll
+    for (int k = 0; k < CPAD; ++k) c[k] = 0.0f;
+    unsigned long long steps_total = 0;
+    const JobDev* J = nullptr;
+    Lane s;
+    int32_t chunk = -1;
+    uint32_t fill = 0;
+    uint32_t g = 0;
+
+    auto fetch = [&]() -> bool {
+        while (true) {
+            const unsigned long long k = atomicAdd(cls.counter, 1ull);
+            if (k >= cls.n_items) return false;
+            uint32_t job, i;
+            if (cls.item_ids != nullptr) {
+                g = cls.item_ids[k];
+                job = upper_bound_u32(mp.job_base, mp.n_jobs + 1, g) - 1;
+                i = g - mp.job_base[job];
+            } else {
+                const uint32_t q = upper_bound_u32(cls.prefix, cls.n_jobs + 1, (uint32_t)k) - 1;
+                job = cls.jobs[q];
+                i = (uint32_t)k - cls.prefix[q];
+                g = mp.job_base[job] + i;
+            }
+            J = mp.jobs + job;
+            const float4 a = J->seeds[2 * (size_t)i];
+            const float4 b = J->seeds[2 * (size_t)i + 1];
+            const uint32_t batch = i / J->batch_size;
+            lane_init(s, a, b, mp.batch_rng_seeds[J->rng_base + batch], i - batch * J->batch_size,
+                      J->seed_offset + i);
+            if (!m_chunk_alloc(mp, chunk)) {
+                mp.first_chunk[g] = -1;
+                mp.lengths[g] = kOverflowBit;
+                continue;
+            }
+            mp.first_chunk[g] = chunk;
+            fill = 0;
+            m_emit(mp, chunk, fill, a.x, a.y, a.z);
+            return true;
+        }
+    };
+
+    bool live = fetch();
+    while (live) {
+        bool done = s.n >= J->t.n_steps;
+        bool overflow = false;
+        if (!done) {
+            float qx, qy, qz;
+            const int r = track_step<MODEL, LMAX, ALGO, CPAD>(J->t, s, c, qx, qy, qz);
+            if (r == 0) {
+                done = true;
+            } else if (r == 2) {
+                if (m_emit(mp, chunk, fill, qx, qy, qz)) {
+                    s.n++;
+                } else {
+                    done = true;
+                    overflow = true;
+                }
+            }
+        }
+        if (done) {
+            mp.lengths[g] = overflow ? (s.n | kOverflowBit) : s.n;
+            if (!overflow) steps_total += s.steps;
+            live = fetch();
+        }
+    }
+    return steps_total;
+}
+
+template <int MODEL, int LMAX, int ALGO>
+__global__ void __launch_bounds__(128) track_class_kernel(const MultiParams mp, const ClassDev cls)
+{
+    const unsigned long long steps = drain_class<MODEL, LMAX, ALGO>(mp, cls);
+    if (steps != 0) atomicAdd(mp.steps_done, steps);
+}
+
+template <int M, int L, int A>
+cudaError_t launch_class(const MultiParams& mp, const ClassDev& cls, int sms, cudaStream_t stream)
+{
+    int blocks = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, track_class_kernel<M, L, A>, 128, 0);
+    if (e != cudaSuccess) return e;
+    const int grid = sms * (blocks > 0 ? blocks : 1);
+    track_class_kernel<M, L, A><<<grid, 128, 0, stream>>>(mp, cls);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_track_class(const MultiParams& mp, const ClassDev& cls, int sms, cudaStream_t s)
+{
+    if (cls.n_items == 0) return cudaSuccess;
+    switch (cls.kind) {
+    case kSH0T: return launch_class<kModelSH, 0, kTransport>(mp, cls, sms, s);
+    case kSH0D: return launch_class<kModelSH, 0, kDiffusion>(mp, cls, sms, s);
+    case kSH2T: return launch_class<kModelSH, 2, kTransport>(mp, cls, sms, s);
+    case kSH2D: return launch_class<kModelSH, 2, kDiffusion>(mp, cls, sms, s);
+    case kSH4T: return launch_class<kModelSH, 4, kTransport>(mp, cls, sms, s);
+    case kSH4D: return launch_class<kModelSH, 4, kDiffusion>(mp, cls, sms, s);
+    case kSH6T: return launch_class<kModelSH, 6, kTransport>(mp, cls, sms, s);
+    case kSH6D: return launch_class<kModelSH, 6, kDiffusion>(mp, cls, sms, s);
+    case kSH8T: return launch_class<kModelSH, 8, kTransport>(mp, cls, sms, s);
+    case kSH8D: return launch_class<kModelSH, 8, kDiffusion>(mp, cls, sms, s);
+    case kDTIT: return launch_class<kModelDTI, 0, kTransport>(mp, cls, sms, s);
+    case kDTID: return launch_class<kModelDTI, 0, kDiffusion>(mp, cls, sms, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace tg

@@ -21,7 +21,12 @@ struct Lane {
     float time;
     uint32_t n;
     RngState rng;
-    int64_t cached;
+    // rounded voxel coordinates of the last domain test and field gather;
+    // while they are unchanged the mask bit (inside) and the coefficients in
+    // registers are still valid, so the bounds tests, index arithmetic and
+    // loads are skipped.  NaN forces the first evaluation.
+    float dvx, dvy, dvz;
+    float fvx, fvy, fvz;
     uint32_t steps;
 };
 
@@ -37,13 +42,16 @@ __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (
     const float ax = dot4(p.dgrid.row0, s.px, s.py, s.pz, 1.0f);
     const float ay = dot4(p.dgrid.row1, s.px, s.py, s.pz, 1.0f);
     const float az = dot4(p.dgrid.row2, s.px, s.py, s.pz, 1.0f);
-    {
-        const float vx = floorf(ax + 0.5f), vy = floorf(ay + 0.5f), vz = floorf(az + 0.5f);
+    const float vx = floorf(ax + 0.5f), vy = floorf(ay + 0.5f), vz = floorf(az + 0.5f);
+    if (vx != s.dvx || vy != s.dvy || vz != s.dvz) {
         if (!(vx >= 0.0f && vx < (float)p.dgrid.nx && vy >= 0.0f && vy < (float)p.dgrid.ny &&
               vz >= 0.0f && vz < (float)p.dgrid.nz))
             return 0;
         const int64_t k = ((int64_t)(int32_t)vx * p.dgrid.ny + (int32_t)vy) * p.dgrid.nz + (int32_t)vz;
         if (__ldg(p.mask + k) == 0) return 0;
+        s.dvx = vx;
+        s.dvy = vy;
+        s.dvz = vz;
     }
     float bx = ax, by = ay, bz = az;
     if (!p.same_grid) {
@@ -52,11 +60,11 @@ __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (
         bz = dot4(p.fgrid.row2, s.px, s.py, s.pz, 1.0f);
     }
     const float fx = rintf(bx), fy = rintf(by), fz = rintf(bz);
-    if (!(fx >= 0.0f && fx < (float)p.fgrid.nx && fy >= 0.0f && fy < (float)p.fgrid.ny &&
-          fz >= 0.0f && fz < (float)p.fgrid.nz))
-        return 0;
-    const int64_t fv = ((int64_t)(int32_t)fx * p.fgrid.ny + (int32_t)fy) * p.fgrid.nz + (int32_t)fz;
-    if (fv != s.cached) {
+    if (fx != s.fvx || fy != s.fvy || fz != s.fvz) {
+        if (!(fx >= 0.0f && fx < (float)p.fgrid.nx && fy >= 0.0f && fy < (float)p.fgrid.ny &&
+              fz >= 0.0f && fz < (float)p.fgrid.nz))
+            return 0;
+        const int64_t fv = ((int64_t)(int32_t)fx * p.fgrid.ny + (int32_t)fy) * p.fgrid.nz + (int32_t)fz;
         const float4* src = reinterpret_cast<const float4*>(p.field) + fv * (CPAD / 4);
 #pragma unroll
         for (int k = 0; k < CPAD / 4; ++k) {
@@ -66,7 +74,9 @@ __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (
             c[4 * k + 2] = v.z;
             c[4 * k + 3] = v.w;
         }
-        s.cached = fv;
+        s.fvx = fx;
+        s.fvy = fy;
+        s.fvz = fz;
     }
 
     update_orientation<MODEL, LMAX, ALGO>(p.algo, c, s.ox, s.oy, s.oz, s.rng);
@@ -97,7 +107,8 @@ __device__ __forceinline__ void lane_init(Lane& s, float4 a, float4 b, uint32_t 
     s.rng.mwc = rng_init(rng_seed, stream_id);
     s.rng.index = index;
     s.rng.step = 0u;
-    s.cached = -1;
+    s.dvx = s.dvy = s.dvz = __int_as_float(0x7fc00000);
+    s.fvx = s.fvy = s.fvz = __int_as_float(0x7fc00000);
     s.steps = 0u;
 }
 

@@ -129,6 +129,11 @@ def _mix(shape, bundles, rng, lmax, isotropic_background):
     weights[covered] /= total[covered, None]
     for b, (member, direction) in enumerate(bundles):
         idx = np.nonzero(member.ravel())[0]
+        if np.ndim(direction) == 1:
+            # one direction for the whole bundle: rotate the kernel once
+            kernel = rotated_kernel(np.asarray(direction, float)[None, :], lmax)[0].astype(np.float32)
+            fod[idx] += weights[idx, b, None].astype(np.float32) * kernel
+            continue
         for start in range(0, len(idx), 262144):
             sel = idx[start: start + 262144]
             fod[sel] += (weights[sel, b, None] * rotated_kernel(direction.reshape(-1, 3)[sel], lmax)).astype(np.float32)
@@ -183,6 +188,66 @@ def config1(seed: int = 0, shape=(145, 174, 145), voxel_mm: float = 1.25, lmax: 
     fod += rng.normal(0.0, 0.01, size=fod.shape).astype(np.float32)
     affine = np.diag([voxel_mm, voxel_mm, voxel_mm, 1.0])
     return Nifti1Image(fod, affine)
+
+
+def bundle_field(shape, lmax: int = 8, seed: int = 0, voxel_mm: float = 2.0):
+    """The config-0 generator at any grid size: bundle A along x everywhere and
+    bundle B on circular arcs in y-z (radius 0.3 of the smaller y/z extent)
+    inside a torus 4 voxels thick; fractions U[0.3, 0.7]; N(0, 0.01) noise.
+    Returns (fod image, ellipsoid mask image with semi-axes 0.45 of each extent)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = shape
+    cy, cz = (ny - 1) / 2.0, (nz - 1) / 2.0
+    i, j, k = np.meshgrid(np.arange(nx, dtype=np.float32), np.arange(ny, dtype=np.float32),
+                          np.arange(nz, dtype=np.float32), indexing="ij")
+    y, z = j - cy, k - cz
+    r = np.hypot(y, z)
+    radius = 0.3 * min(ny, nz)
+    torus = np.abs(r - radius) < 2.0
+    with np.errstate(invalid="ignore", divide="ignore"):
+        rr = np.where(r > 0, r, 1)
+        dir_b = np.stack([np.zeros_like(r), -z / rr, y / rr], axis=-1)
+    bundles = [(np.ones(shape, bool), np.array([1.0, 0.0, 0.0])), (torus, dir_b)]
+    fod = _mix(tuple(shape), bundles, rng, lmax, isotropic_background=False)
+    fod += rng.normal(0.0, 0.01, size=fod.shape).astype(np.float32)
+    affine = np.diag([voxel_mm, voxel_mm, voxel_mm, 1.0])
+    cx = (nx - 1) / 2.0
+    mask = (((i - cx) / (0.45 * nx)) ** 2 + ((j - cy) / (0.45 * ny)) ** 2 + ((k - cz) / (0.45 * nz)) ** 2) <= 1.0
+    return Nifti1Image(fod.astype(np.float32), affine), Nifti1Image(mask.astype(np.uint8), affine)
+
+
+MIXED_SHAPES = ((64, 64, 64), (96, 96, 60), (128, 128, 128), (145, 174, 145))
+
+
+def mixed_job_specs(n_jobs: int = 64, seed: int = 0, max_seeds: int = 500_000, min_seeds: int = 1000):
+    """Config-3 job draws: volume size, lmax (4/6/8), seed count log-U[1k, 500k],
+    Transport or Diffusion (noise variance U[0.05, 0.2]), maximum length U[50, 300] mm."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(n_jobs):
+        specs.append({
+            "shape": MIXED_SHAPES[int(rng.integers(0, len(MIXED_SHAPES)))],
+            "lmax": int(rng.choice([4, 6, 8])),
+            "n_seeds": int(np.exp(rng.uniform(np.log(min_seeds), np.log(max_seeds)))),
+            "algorithm": "transport" if rng.uniform() < 0.5 else "diffusion",
+            "noise_variance": float(rng.uniform(0.05, 0.2)),
+            "max_length": float(rng.uniform(50.0, 300.0)),
+            "seed": int(rng.integers(0, 2 ** 31)),
+        })
+    return specs
+
+
+def uniform_seeds(mask_img, n: int, seed: int = 0) -> np.ndarray:
+    """n seeds uniform in the mask's nonzero voxels with uniform orientations."""
+    rng = np.random.default_rng(seed)
+    vox = np.argwhere(np.asarray(mask_img.dataobj) != 0)
+    pick = vox[rng.integers(0, len(vox), n)] + rng.uniform(-0.5, 0.5, (n, 3))
+    loc = pick @ np.asarray(mask_img.affine)[:3, :3].T + np.asarray(mask_img.affine)[:3, 3]
+    o = rng.normal(size=(n, 3))
+    o /= np.linalg.norm(o, axis=1, keepdims=True)
+    out = np.empty((n, 8), np.float32)
+    out[:, :3], out[:, 3], out[:, 4:7], out[:, 7] = loc, 1.0, o, 0.0
+    return out
 
 
 def dti_field(shape=(96, 96, 60), seed: int = 0, voxel_mm: float = 2.0):
