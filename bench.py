@@ -77,8 +77,8 @@ def parse_args():
     p.add_argument("--seeds", type=int, default=1000000, help="seeds per step (one tg.tractogram job)")
     p.add_argument("--batch", type=int, default=50000, help="reference batch_size inside a job")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["config1", "mixed"], default="config1",
-                   help="config1 (default headline) or the 64-job mixed workload")
+    p.add_argument("--workload", choices=["config1", "mixed", "config2"], default="config1",
+                   help="config1 (default headline), the 64-job mixed workload, or the DTI + mesh workload")
     p.add_argument("--jobs", type=int, default=64, help="jobs of the mixed workload")
     return p.parse_args()
 
@@ -583,12 +583,150 @@ def run_mixed(args):
     print(json.dumps(line), flush=True)
 
 
+C2_STEP = 0.2           # 0.1 voxel at 2 mm
+C2_SEEDS = 2_000_000
+C2_BYTES_PER_STEP = 4 * 6 + 1 + 16 * C2_STEP / SAVE_AT
+C2_WORKLOAD = ("config2 DTI + mesh: 96x96x60 tensors (6 f32) at 2 mm along the config-0 field with 5% "
+               "log-normal eigenvalue jitter; closed surface of 499280 triangles (geodesic sphere, "
+               "r = 1 + 0.1 Y21 + 0.05 Y40, scaled to the volume) terminating streamlines through its BVH; "
+               "2M seeds uniform inside; Transport, step 0.2 mm (0.1 voxel), gamma 1; save_at 0.25, "
+               "max length 300 mm; batches of 50000")
+
+
+def setup_config2(runtime, n_seeds):
+    import tractography_b200 as tg
+    from tractography_b200 import synthetic
+
+    fod = synthetic.dti_field(shape=(96, 96, 60), seed=0)
+    field = tg.field.Image(fod)
+    v, f = synthetic.config2_surface()
+    mesh = tg.domain.Mesh(v, f)
+    seeds = synthetic.seeds_inside(lambda p: tg.domain.contains(mesh, p, runtime), v.min(axis=0), v.max(axis=0),
+                                   n_seeds, seed=5)
+    algorithm = tg.algorithm.Transport(tg.local.DiffusionTensorImaging(), step_size=C2_STEP, gamma=1.0)
+    return field, mesh, seeds, algorithm
+
+
+def run_config2(args):
+    """Config 2: DTI Transport in a closed-surface (BVH) domain, 2M seeds."""
+    import torch
+
+    import tractography_b200 as tg
+    from tractography_b200 import _lib
+    from tractography_b200.algorithm import to_struct
+
+    torch.cuda.set_device(0)
+    runtime = tg.CudaRuntime(0)
+    lib = runtime.lib
+    sh = ctypes.c_void_p(runtime.stream_handle)
+    n_job = args.seeds if args.seeds != 1000000 else C2_SEEDS
+    field, mesh, seeds, algorithm = setup_config2(runtime, n_job)
+    n_steps = int(math.floor(MAX_LENGTH / SAVE_AT))
+    n_batches = (n_job + args.batch - 1) // args.batch
+    rng = np.zeros(n_batches, np.uint32)
+    with runtime.device_scope():
+        d_handle = mesh.device(runtime)
+        f_handle = field.device(runtime, _lib.MODEL_DTI)
+        tracker = runtime.tracker()
+        a = to_struct(algorithm)
+        dev_seeds = runtime.to_device(seeds)
+        host_seeds = runtime.pinned(seeds.shape, np.float32)
+        host_seeds[...] = seeds
+        lengths = np.empty(n_job, np.uint32)
+        offsets = np.empty(n_job, np.uint64)
+        total, steps = ctypes.c_uint64(), ctypes.c_uint64()
+        kms, waves, launches = ctypes.c_float(), ctypes.c_uint32(), ctypes.c_uint32()
+
+        def run(on_host):
+            ptr = host_seeds.ctypes.data_as(ctypes.c_void_p) if on_host else ctypes.c_void_p(dev_seeds.data_ptr())
+            _lib.check(lib.tg_tracker_run(tracker, ctypes.byref(a), d_handle, f_handle, ptr, 1 if on_host else 0,
+                                          n_job, args.batch, rng.ctypes.data_as(ctypes.c_void_p), SAVE_AT, n_steps,
+                                          lengths.ctypes.data_as(ctypes.c_void_p),
+                                          offsets.ctypes.data_as(ctypes.c_void_p), ctypes.byref(total),
+                                          ctypes.byref(steps), sh))
+            _lib.check(lib.tg_tracker_stats(tracker, ctypes.byref(kms), ctypes.byref(waves), ctypes.byref(launches)))
+            return int(steps.value), int(total.value), float(kms.value), int(launches.value)
+
+        warm = 0
+        for _ in range(args.warmup):
+            warm = max(warm, run(False)[1])
+        out_host = runtime.pinned((int(warm * 1.25) + 1024, 3), np.float32)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(0)
+        with sampler:
+            torch.cuda.synchronize()
+            ev0.record(runtime.stream)
+            dev_steps = dev_points = n_launch = 0
+            kernel_ms = 0.0
+            for _ in range(args.steps):
+                st, pts, k, nl = run(False)
+                dev_steps, dev_points, kernel_ms, n_launch = dev_steps + st, dev_points + pts, kernel_ms + k, \
+                    n_launch + nl
+            ev1.record(runtime.stream)
+            torch.cuda.synchronize()
+            dev_ms = ev0.elapsed_time(ev1)
+            ev0.record(runtime.stream)
+            e2e_steps = h2d = d2h = 0
+            for _ in range(args.steps):
+                st, pts, _, _ = run(True)
+                if pts > out_host.shape[0]:
+                    out_host = runtime.pinned((pts, 3), np.float32)
+                _lib.check(lib.tg_tracker_copy_points(tracker, out_host.ctypes.data_as(ctypes.c_void_p), 0, pts, 1,
+                                                      sh))
+                e2e_steps += st
+                h2d += seeds.nbytes + rng.nbytes
+                d2h += pts * 12 + n_job * 12
+            ev1.record(runtime.stream)
+            torch.cuda.synchronize()
+            e2e_ms = ev0.elapsed_time(ev1)
+    peak, peak_kind = measured_peaks()
+    kernel_sps = dev_steps / (kernel_ms / 1e3)
+    info = mesh.info(runtime)
+    line = {
+        "metric": METRIC, "value": dev_steps / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator; no dataset)",
+        "workload": "config2",
+        "config": {"workload": C2_WORKLOAD, "seeds_per_step": n_job, "batch_size": args.batch,
+                   "mesh": info, "cache": "BVH (34 MB) and tensor volume (13 MB) are L2-resident by design"},
+        "streamlines_per_s": n_job * args.steps / (dev_ms / 1e3),
+        "points_per_step": dev_points / args.steps,
+        "e2e": {"value": e2e_steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d / args.steps),
+                "d2h_bytes_per_step": int(d2h / args.steps)},
+        "gpu_launches": n_launch,
+        "roofline": {"bound": "hbm", "achieved": kernel_sps * C2_BYTES_PER_STEP / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": kernel_sps * C2_BYTES_PER_STEP / 1e9 / peak, "traffic": None,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "bytes_per_step": C2_BYTES_PER_STEP,
+                     "note": "bytes exclude the BVH nodes and triangles read near the surface",
+                     "kernel_ms_per_step": kernel_ms / args.steps},
+        "clocks": sampler.summary(),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        threads = os.cpu_count() or 1
+        n_sample = min(n_job, 200 * threads)
+        case = O.Case(field=field.values, field_inv_affine=field.inverse_affine, model=O.MODEL_DTI,
+                      algorithm=O.ALGO_TRANSPORT, step_size=C2_STEP, gamma=1.0, save_at=SAVE_AT, n_steps=n_steps,
+                      mesh=O.BoundaryBvh.build(mesh.vertices, mesh.faces))
+        t0 = time.perf_counter()
+        _, _, st = case.tractogram(seeds[:n_sample], n_threads=threads, return_steps=True)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": st / dt, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"first {n_sample} seeds ({st} steps, {dt:.1f} s); plain-C oracle with "
+                                          "the reference's BVH traversal, OpenMP over seeds"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "mixed":
         run_mixed(args)
+    elif args.workload == "config2":
+        run_config2(args)
     else:
         run_ours(args)
 

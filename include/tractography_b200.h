@@ -94,6 +94,45 @@ int tg_domain_create(const uint8_t* mask, uint32_t nx, uint32_t ny, uint32_t nz,
                      const float inverse_affine[16], void* stream, tg_domain** out);
 int tg_domain_destroy(tg_domain* domain);
 
+/* Closed triangle surface as a tracking domain.  The reference builds a
+ * boundary mesh and its BVH for every domain (BaseDomain._set_boundary_data,
+ * domain.py:44-116) and traverses it with bvh_segment_hit (utils/bvh.cl:
+ * 83-131); this entry point makes such a surface the domain itself: a seed
+ * is inside by a three-ray crossing-parity vote and a streamline stops at
+ * the first step whose segment from the previous point hits the surface.
+ * `vertices` (n_vertices, 3) float64 and `faces` (n_faces, 3) are host
+ * arrays; faces wound outward.  The BVH is built on the host (median split
+ * of domain.py:72-116) and stays resident with a distance grid that lets
+ * steps far from the surface skip the traversal without changing a result.
+ * Mesh domains are accepted by tg_tractogram, tg_tractogram_host,
+ * tg_tracker_run and tg_domain_contains (not by tg_tracker_run_jobs or
+ * tg_tractogram_noalloc, which return TG_ERR_UNSUPPORTED). */
+int tg_domain_create_mesh(const double* vertices, uint32_t n_vertices, const uint32_t* faces,
+                          uint32_t n_faces, void* stream, tg_domain** out);
+
+/* The boundary BVH of domain.py:72-116 built on the host only, in the
+ * reference's array layout (no device needed).  Call with null arrays to
+ * get n_triangles (non-degenerate faces kept) and n_nodes; then with
+ * arrays of (n_vertices, 4) float, (n_triangles, 4) uint32, (n_nodes, 4)
+ * float bounds_min / bounds_max, (n_nodes, 4) int32 nodes and
+ * (n_triangles,) ordered triangle ids. */
+int tg_bvh_build_host(const double* vertices, uint32_t n_vertices, const uint32_t* faces,
+                      uint32_t n_faces, uint32_t* n_triangles, uint32_t* n_nodes, float* vertices4,
+                      uint32_t* triangles4, float* bounds_min, float* bounds_max, int32_t* nodes,
+                      uint32_t* ordered_triangles);
+
+/* Size of a mesh domain: triangles, BVH nodes, distance-grid cells per axis
+ * and device bytes held. */
+int tg_mesh_info(const tg_domain* domain, uint32_t* n_triangles, uint32_t* n_nodes, uint32_t grid[3],
+                 uint64_t* device_bytes);
+
+/* bvh_segment_hit (utils/bvh.cl:83-131) per segment: device arrays
+ * starts/ends (n, 4) float32; writes found (n) uint8, triangle (n) uint32
+ * (index among the kept faces) and hit (n, 4) = barycentric (1-u-v, u, v)
+ * and the segment parameter t. */
+int tg_mesh_segment_hits(const tg_domain* domain, const float* starts, const float* ends, uint32_t n,
+                         uint8_t* found, uint32_t* triangle, float* hit, void* stream);
+
 /* The reference kernel contract (tracking.py:93-176): one launch over
  * n_seeds device seeds; writes the dense (n_seeds, n_steps, 4) float32
  * points and uint32 lengths to device memory exactly as the reference's
@@ -161,6 +200,19 @@ int tg_tracker_run_jobs(tg_tracker* tracker, const tg_job* jobs, uint32_t n_jobs
  * than one only when the point pool ran out) and number of kernel launches.
  * No reference counterpart: instrumentation for the benchmark. */
 int tg_tracker_stats(const tg_tracker* tracker, float* kernel_ms, uint32_t* waves, uint32_t* launches);
+
+/* Launch shape and tail compaction of the tracker's persistent launches.
+ * blocks_per_sm: resident blocks of 128 lanes per SM (0 = the occupancy
+ * maximum; larger values are capped to it).  Tail compaction: once a launch's
+ * queue is empty, a warp with at most compact_lanes live streamlines hands
+ * them to the next round and exits; compact_rounds further rounds run those
+ * streamlines in full warps, the last round to completion (compact_lanes 0:
+ * one launch, no compaction).  Results do not depend on these settings.
+ * Defaults: 0, 8, 4.  No reference counterpart: the autotuner's knobs. */
+int tg_tracker_set_tuning(tg_tracker* tracker, uint32_t blocks_per_sm, uint32_t compact_lanes,
+                          uint32_t compact_rounds);
+int tg_tracker_get_tuning(const tg_tracker* tracker, uint32_t* blocks_per_sm, uint32_t* compact_lanes,
+                          uint32_t* compact_rounds);
 
 /* Copy points [first, first + count) of the packed (total_points, 3)
  * float32 buffer of the last run to `dst` (host when dst_on_host != 0). */

@@ -13,6 +13,8 @@ becomes a run-time value, and one counter increment is inserted before the
 orientation update so accepted steps can be counted.  oracle/clshim.hpp
 supplies the OpenCL built-ins.  g++ compiles each variant in its own
 translation unit and namespace; the outputs go only to oracle/_ref/.
+The boundary BVH traversal (utils/bvh.cl) is compiled the same way with a
+batch driver, for the BVH hit parity tests.
 
 Nothing from the reference is copied into this repository: the sources are
 read from the reference tree at build time.
@@ -199,6 +201,37 @@ extern "C" void tgref_update_{name}(float step, float gamma, float noise, unsign
 """
 
 
+BVH_DRIVER = """
+extern "C" void tgref_bvh_hits(const float* vertices, const unsigned int* triangles, const float* bounds_min,
+        const float* bounds_max, const int* nodes, const unsigned int* ordered, unsigned int n_nodes,
+        const float* starts, const float* ends, unsigned int n, unsigned char* found, unsigned int* triangle,
+        float* hit)
+{
+    const bvhref::BVH bvh = {(const float4*)vertices, (const uint4*)triangles, (const float4*)bounds_min,
+                             (const float4*)bounds_max, (const int4*)nodes, ordered, n_nodes};
+    for (unsigned int i = 0; i < n; ++i) {
+        const float3 s = make_float3(starts[4 * i], starts[4 * i + 1], starts[4 * i + 2]);
+        const float3 e = make_float3(ends[4 * i], ends[4 * i + 1], ends[4 * i + 2]);
+        unsigned int tri = 0;
+        float3 bc = make_float3(0.0f, 0.0f, 0.0f);
+        float t = 1.0f;
+        found[i] = bvhref::bvh_segment_hit(bvh, s, e, &tri, &bc, &t) ? 1 : 0;
+        triangle[i] = tri;
+        hit[4 * i] = bc.x;
+        hit[4 * i + 1] = bc.y;
+        hit[4 * i + 2] = bc.z;
+        hit[4 * i + 3] = t;
+    }
+}
+"""
+
+
+def bvh_source(kernel_dir):
+    """utils/bvh.cl (the boundary BVH traversal) as C++ with a batch driver."""
+    text = rewrite_literals(inline_includes((kernel_dir / "utils" / "bvh.cl").read_text(), kernel_dir))
+    return f'#include "clshim.hpp"\nnamespace bvhref {{\n{text}\n}}\n' + BVH_DRIVER
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -230,6 +263,9 @@ def main():
         upath = OUT / f"tgref_{uname}.cpp"
         upath.write_text(ucpp)
         sources.append(upath)
+    bpath = OUT / "tgref_bvh.cpp"
+    bpath.write_text(bvh_source(kernel_dir))
+    sources.append(bpath)
     flags = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-march=x86-64-v3",
              "-mtune=generic", "-w", f"-I{HERE}"]
     procs = []

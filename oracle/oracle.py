@@ -40,6 +40,19 @@ class Problem(ctypes.Structure):
         ("seed_offset", ctypes.c_uint64),
         ("save_at", ctypes.c_float),
         ("n_steps", ctypes.c_uint32),
+        ("mesh", ctypes.c_void_p),
+    ]
+
+
+class Bvh(ctypes.Structure):
+    _fields_ = [
+        ("vertices", ctypes.c_void_p),
+        ("triangles", ctypes.c_void_p),
+        ("bounds_min", ctypes.c_void_p),
+        ("bounds_max", ctypes.c_void_p),
+        ("nodes", ctypes.c_void_p),
+        ("ordered_triangles", ctypes.c_void_p),
+        ("n_nodes", ctypes.c_uint32),
     ]
 
 
@@ -71,6 +84,11 @@ def lib():
         _lib.tgo_randi_stream.argtypes = [U32, U32, U32, U32, P]
         _lib.tgo_philox.argtypes = [P, P, P]
         _lib.tgo_math.argtypes = [ctypes.c_int, P, U32, P]
+        _lib.tgo_segment_hits.argtypes = [P, P, P, U32, P, P, P, ctypes.c_int]
+        _lib.tgo_mesh_contains.argtypes = [P, F, F, F]
+        _lib.tgo_mesh_contains.restype = ctypes.c_int
+        _lib.tgo_bvh_count_hits.argtypes = [P, P, P]
+        _lib.tgo_bvh_count_hits.restype = U32
     return _lib
 
 
@@ -84,8 +102,11 @@ class Case:
     def __init__(self, *, mask=None, mask_inv_affine=None, field=None, field_inv_affine=None,
                  model=MODEL_SH, algorithm=ALGO_TRANSPORT, step_size=0.001, gamma=1.0,
                  noise_variance=0.0, rng_mode=RNG_MWC64X, rng_seed=0, philox_key=0,
-                 seed_offset=0, save_at=1.0, n_steps=0):
+                 seed_offset=0, save_at=1.0, n_steps=0, mesh=None):
         self.p = Problem()
+        if mesh is not None:
+            self.mesh = mesh
+            self.p.mesh = ctypes.addressof(mesh.struct)
         if mask is not None:
             self.mask = np.ascontiguousarray(mask != 0, dtype=np.int32)
             self.p.mask = self.mask.ctypes.data
@@ -139,7 +160,8 @@ class Case:
 
 
 def _points4(points, w=1.0):
-    points = np.asarray(points, dtype=np.float32).reshape(-1, points.shape[-1] if np.ndim(points) > 1 else 3)
+    points = np.asarray(points, dtype=np.float32)
+    points = points.reshape(-1, points.shape[-1] if points.ndim > 1 else 3)
     out = np.full((len(points), 4), w, dtype=np.float32)
     out[:, :3] = points[:, :3]
     return out
@@ -203,3 +225,91 @@ def math(which, x):
     code = {"sin": 0, "cos": 1, "exp": 2, "log": 3}[which]
     lib().tgo_math(code, _ptr(x), x.size, _ptr(out))
     return out
+
+
+# ---------------------------------------------------------------- boundary BVH
+
+class BoundaryBvh:
+    """A triangle surface and its BVH in the reference's array layout.
+
+    ``build`` restates BaseDomain._set_boundary_data (domain.py:44-116):
+    degenerate (zero or non-finite area) triangles are dropped, triangle
+    bounds and centroids are float64, each node splits its triangles at the
+    median of the centroids along the longest axis of its bounds (first axis
+    on ties) after sorting them by that centroid coordinate, leaves hold at
+    most 4 triangles, nodes are numbered in preorder and bounds are stored as
+    float32.  The sort here is stable; NumPy's default argsort in the
+    reference is not, so the two orders agree whenever no two centroids of a
+    node are equal along its split axis.
+    """
+
+    LEAF_SIZE = 4
+
+    def __init__(self, vertices4, triangles4, bounds_min, bounds_max, nodes, ordered):
+        self.vertices = np.ascontiguousarray(vertices4, np.float32)
+        self.triangles = np.ascontiguousarray(triangles4, np.uint32)
+        self.bounds_min = np.ascontiguousarray(bounds_min, np.float32)
+        self.bounds_max = np.ascontiguousarray(bounds_max, np.float32)
+        self.nodes = np.ascontiguousarray(nodes, np.int32)
+        self.ordered = np.ascontiguousarray(ordered, np.uint32)
+        self.struct = Bvh(self.vertices.ctypes.data, self.triangles.ctypes.data, self.bounds_min.ctypes.data,
+                          self.bounds_max.ctypes.data, self.nodes.ctypes.data, self.ordered.ctypes.data,
+                          len(self.nodes))
+
+    @classmethod
+    def build(cls, vertices, faces):
+        vertices = np.asarray(vertices, dtype=np.float64)
+        faces = np.asarray(faces, dtype=np.uint32)
+        tv = vertices[faces]
+        area = 0.5 * np.linalg.norm(np.cross(tv[:, 1] - tv[:, 0], tv[:, 2] - tv[:, 0]), axis=1)
+        faces = faces[np.isfinite(area) & (area > 0)]
+        tv = vertices[faces]
+        tmin, tmax = tv.min(axis=1), tv.max(axis=1)
+        centroid = (tmin + tmax) * 0.5
+        node_lo, node_hi, node_data, ordered = [], [], [], []
+
+        def split(ids):
+            me = len(node_data)
+            node_lo.append(None)
+            node_hi.append(None)
+            node_data.append(None)
+            lo, hi = tmin[ids].min(axis=0), tmax[ids].max(axis=0)
+            if len(ids) <= cls.LEAF_SIZE:
+                node_data[me] = (-1, -1, len(ordered), len(ids))
+                ordered.extend(int(i) for i in ids)
+            else:
+                axis = int(np.argmax(hi - lo))
+                ids = ids[np.argsort(centroid[ids, axis], kind="stable")]
+                half = len(ids) // 2
+                left = split(ids[:half])
+                right = split(ids[half:])
+                node_data[me] = (left, right, 0, 0)
+            node_lo[me], node_hi[me] = lo, hi
+            return me
+
+        split(np.arange(len(faces), dtype=np.int64))
+        v4 = np.ones((len(vertices), 4), np.float32)
+        v4[:, :3] = vertices
+        t4 = np.zeros((len(faces), 4), np.uint32)
+        t4[:, :3] = faces
+        bmin = np.zeros((len(node_lo), 4), np.float32)
+        bmax = np.zeros((len(node_hi), 4), np.float32)
+        bmin[:, :3] = np.asarray(node_lo)
+        bmax[:, :3] = np.asarray(node_hi)
+        return cls(v4, t4, bmin, bmax, np.asarray(node_data, np.int32), np.asarray(ordered, np.uint32))
+
+    def segment_hits(self, starts, ends, n_threads=1):
+        """bvh.cl:83-131 per row: (found, triangle, (n, 4) barycentric xyz + t)."""
+        s4, e4 = _points4(starts), _points4(ends)
+        n = len(s4)
+        found = np.zeros(n, np.uint8)
+        tri = np.zeros(n, np.uint32)
+        hit = np.zeros((n, 4), np.float32)
+        lib().tgo_segment_hits(ctypes.byref(self.struct), _ptr(s4), _ptr(e4), n, _ptr(found), _ptr(tri), _ptr(hit),
+                               n_threads)
+        return found.astype(bool), tri, hit
+
+    def contains(self, points):
+        pts = np.asarray(points, np.float32).reshape(-1, 3)
+        f = lib().tgo_mesh_contains
+        return np.array([f(ctypes.byref(self.struct), *map(float, q)) for q in pts], dtype=bool)

@@ -89,3 +89,25 @@ def update_orientation(model, n_coefficients, algorithm, step_size, gamma, noise
     fn(step_size, gamma, noise_variance, rng_seed & 0xFFFFFFFF, params.ctypes.data, o4.ctypes.data, len(o4),
        out.ctypes.data)
     return out[:, :3]
+
+
+def bvh_hits(vertices4, triangles4, bounds_min, bounds_max, nodes, ordered, starts, ends):
+    """The reference's bvh_segment_hit (utils/bvh.cl:83-131) per segment.
+
+    Returns (found, triangle, (n, 4) barycentric xyz + t)."""
+    arrays = [np.ascontiguousarray(a, dt) for a, dt in ((vertices4, np.float32), (triangles4, np.uint32),
+                                                        (bounds_min, np.float32), (bounds_max, np.float32),
+                                                        (nodes, np.int32), (ordered, np.uint32))]
+    s4 = np.zeros((len(starts), 4), np.float32)
+    e4 = np.zeros((len(ends), 4), np.float32)
+    s4[:, :3], e4[:, :3] = np.asarray(starts)[:, :3], np.asarray(ends)[:, :3]
+    n = len(s4)
+    found = np.zeros(n, np.uint8)
+    tri = np.zeros(n, np.uint32)
+    hit = np.zeros((n, 4), np.float32)
+    fn = lib().tgref_bvh_hits
+    P = ctypes.c_void_p
+    fn.argtypes = [P] * 6 + [ctypes.c_uint, P, P, ctypes.c_uint, P, P, P]
+    fn(*[a.ctypes.data for a in arrays], len(arrays[4]), s4.ctypes.data, e4.ctypes.data, n, found.ctypes.data,
+       tri.ctypes.data, hit.ctypes.data)
+    return found.astype(bool), tri, hit

@@ -377,6 +377,182 @@ static const float* field_voxel(const tgo_problem* p, float x, float y, float z)
 }
 
 /* ------------------------------------------------------------------ */
+/* Boundary BVH: bvh.cl:16-131                                          */
+/* ------------------------------------------------------------------ */
+
+static float cl_minf(float x, float y) { return (y < x) ? y : x; }
+
+static float dot3(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+static void cross3(const float* a, const float* b, float* r)
+{
+    r[0] = a[1] * b[2] - a[2] * b[1];
+    r[1] = a[2] * b[0] - a[0] * b[2];
+    r[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* bvh.cl:16-45: slab test of the segment start + t * direction, t in [0, max_t]. */
+static int bounds_hit(const tgo_bvh* b, uint32_t node, const float* start, const float* dir, float max_t)
+{
+    float t_lo = 0.0f, t_hi = max_t;
+    const float* lo = b->bounds_min + 4 * (size_t)node;
+    const float* hi = b->bounds_max + 4 * (size_t)node;
+    for (int a = 0; a < 3; ++a) {
+        if (fabsf(dir[a]) < 1e-12f) {
+            if (start[a] < lo[a] || start[a] > hi[a]) return 0;
+            continue;
+        }
+        const float inv = 1.0f / dir[a];
+        float t0 = (lo[a] - start[a]) * inv;
+        float t1 = (hi[a] - start[a]) * inv;
+        if (t0 > t1) {
+            const float tmp = t0;
+            t0 = t1;
+            t1 = tmp;
+        }
+        t_lo = cl_maxf(t_lo, t0);
+        t_hi = cl_minf(t_hi, t1);
+        if (t_lo > t_hi) return 0;
+    }
+    return 1;
+}
+
+/* bvh.cl:47-80: Moller-Trumbore with the reference's tolerances. */
+static int triangle_hit(const tgo_bvh* b, uint32_t tri, const float* start, const float* dir, float max_t,
+                        float* t_out, float* bary)
+{
+    const uint32_t* ix = b->triangles + 4 * (size_t)tri;
+    const float* A = b->vertices + 4 * (size_t)ix[0];
+    const float* B = b->vertices + 4 * (size_t)ix[1];
+    const float* Cv = b->vertices + 4 * (size_t)ix[2];
+    const float e1[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]};
+    const float e2[3] = {Cv[0] - A[0], Cv[1] - A[1], Cv[2] - A[2]};
+    float pv[3], qv[3];
+    cross3(dir, e2, pv);
+    const float det = dot3(e1, pv);
+    if (fabsf(det) < 1e-10f) return 0;
+    const float inv_det = 1.0f / det;
+    const float off[3] = {start[0] - A[0], start[1] - A[1], start[2] - A[2]};
+    const float u = dot3(off, pv) * inv_det;
+    if (u < -1e-6f || u > 1.0f + 1e-6f) return 0;
+    cross3(off, e1, qv);
+    const float v = dot3(dir, qv) * inv_det;
+    if (v < -1e-6f || u + v > 1.0f + 1e-6f) return 0;
+    const float t = dot3(e2, qv) * inv_det;
+    if (t <= 1e-6f || t > max_t) return 0;
+    *t_out = t;
+    bary[0] = 1.0f - u - v;
+    bary[1] = u;
+    bary[2] = v;
+    return 1;
+}
+
+/* bvh.cl:83-131: depth-first with an explicit 64-entry stack, left child
+ * popped first, closest hit kept (a later hit at equal t replaces it). */
+int tgo_bvh_segment_hit(const tgo_bvh* b, const float start[3], const float end[3], uint32_t* triangle,
+                        float barycentric[3], float* t)
+{
+    const float dir[3] = {end[0] - start[0], end[1] - start[1], end[2] - start[2]};
+    int32_t stack[64];
+    uint32_t depth = 1;
+    stack[0] = 0;
+    *t = 1.0f;
+    *triangle = 0;
+    int found = 0;
+    while (depth > 0) {
+        const uint32_t node = (uint32_t)stack[--depth];
+        if (!bounds_hit(b, node, start, dir, *t)) continue;
+        const int32_t* nd = b->nodes + 4 * (size_t)node;
+        if (nd[3] > 0) {
+            for (int32_t i = 0; i < nd[3]; ++i) {
+                const uint32_t tri = b->ordered_triangles[nd[2] + i];
+                float tt, bc[3];
+                if (triangle_hit(b, tri, start, dir, *t, &tt, bc)) {
+                    *t = tt;
+                    *triangle = tri;
+                    barycentric[0] = bc[0];
+                    barycentric[1] = bc[1];
+                    barycentric[2] = bc[2];
+                    found = 1;
+                }
+            }
+        } else {
+            if (depth + 2 > 64) return found;
+            stack[depth++] = nd[1];
+            stack[depth++] = nd[0];
+        }
+    }
+    return found;
+}
+
+uint32_t tgo_bvh_count_hits(const tgo_bvh* b, const float start[3], const float end[3])
+{
+    const float dir[3] = {end[0] - start[0], end[1] - start[1], end[2] - start[2]};
+    int32_t stack[64];
+    uint32_t depth = 1, hits = 0;
+    stack[0] = 0;
+    while (depth > 0) {
+        const uint32_t node = (uint32_t)stack[--depth];
+        if (!bounds_hit(b, node, start, dir, 1.0f)) continue;
+        const int32_t* nd = b->nodes + 4 * (size_t)node;
+        if (nd[3] > 0) {
+            for (int32_t i = 0; i < nd[3]; ++i) {
+                float tt, bc[3];
+                hits += (uint32_t)triangle_hit(b, b->ordered_triangles[nd[2] + i], start, dir, 1.0f, &tt, bc);
+            }
+        } else {
+            if (depth + 2 > 64) return hits;
+            stack[depth++] = nd[1];
+            stack[depth++] = nd[0];
+        }
+    }
+    return hits;
+}
+
+/* Three fixed ray directions of the closed-surface inside test (unit
+ * length to float precision, chosen off every coordinate plane and
+ * diagonal so that rays rarely meet mesh edges). */
+static const float kMeshRays[3][3] = {
+    {0.53896236f, 0.77412713f, 0.33221170f},
+    {-0.68169260f, 0.22392839f, 0.69653570f},
+    {0.17420970f, -0.54785200f, 0.81824590f},
+};
+
+int tgo_mesh_contains(const tgo_bvh* b, float x, float y, float z)
+{
+    const float p[3] = {x, y, z};
+    const float* lo = b->bounds_min;
+    const float* hi = b->bounds_max;
+    for (int a = 0; a < 3; ++a)
+        if (!(p[a] >= lo[a] && p[a] <= hi[a])) return 0;
+    const float reach = (((hi[0] - lo[0]) + (hi[1] - lo[1])) + (hi[2] - lo[2])) + 1.0f;
+    int odd = 0;
+    for (int r = 0; r < 3; ++r) {
+        const float e[3] = {p[0] + reach * kMeshRays[r][0], p[1] + reach * kMeshRays[r][1],
+                            p[2] + reach * kMeshRays[r][2]};
+        odd += (int)(tgo_bvh_count_hits(b, p, e) & 1u);
+    }
+    return odd >= 2;
+}
+
+void tgo_segment_hits(const tgo_bvh* b, const float* starts, const float* ends, uint32_t n, uint8_t* found,
+                      uint32_t* triangle, float* hit, int n_threads)
+{
+    long i;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(n_threads > 0 ? n_threads : 1)
+    for (i = 0; i < (long)n; ++i) {
+        float t = 1.0f, bc[3] = {0.0f, 0.0f, 0.0f};
+        uint32_t tri = 0;
+        found[i] = (uint8_t)tgo_bvh_segment_hit(b, starts + 4 * i, ends + 4 * i, &tri, bc, &t);
+        triangle[i] = tri;
+        hit[4 * i] = bc[0];
+        hit[4 * i + 1] = bc[1];
+        hit[4 * i + 2] = bc[2];
+        hit[4 * i + 3] = t;
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* Tracking loop: tracking.py:105-148                                  */
 /* ------------------------------------------------------------------ */
 
@@ -394,8 +570,26 @@ static uint32_t track_one(const tgo_problem* p, const float* seed, uint32_t gid,
     out[0] = seed[0]; out[1] = seed[1]; out[2] = seed[2]; out[3] = seed[3];
     uint32_t n = 1;
     float time = 0.0f;
+    float last[3] = {pos[0], pos[1], pos[2]};
+    int first = 1;
     while (n < n_steps) {
-        if (!domain_contains(p, pos[0], pos[1], pos[2])) break;
+        if (p->mesh) {
+            /* closed surface: the seed must be inside, each later point is
+             * reached by a segment that does not hit the surface */
+            if (first) {
+                if (!tgo_mesh_contains(p->mesh, pos[0], pos[1], pos[2])) break;
+            } else {
+                uint32_t tri;
+                float bc[3], t;
+                if (tgo_bvh_segment_hit(p->mesh, last, pos, &tri, bc, &t)) break;
+            }
+            first = 0;
+            last[0] = pos[0];
+            last[1] = pos[1];
+            last[2] = pos[2];
+        } else if (!domain_contains(p, pos[0], pos[1], pos[2])) {
+            break;
+        }
         const float* c = field_voxel(p, pos[0], pos[1], pos[2]);
         if (!c) break;
         update_orientation(p, c, C, o, &rng);
@@ -439,7 +633,8 @@ uint64_t tgo_tractogram(const tgo_problem* p, const float* seeds, uint32_t n_see
 void tgo_contains(const tgo_problem* p, const float* points, uint32_t n, uint8_t* out)
 {
     for (uint32_t i = 0; i < n; ++i)
-        out[i] = (uint8_t)domain_contains(p, points[4 * i], points[4 * i + 1], points[4 * i + 2]);
+        out[i] = (uint8_t)(p->mesh ? tgo_mesh_contains(p->mesh, points[4 * i], points[4 * i + 1], points[4 * i + 2])
+                                   : domain_contains(p, points[4 * i], points[4 * i + 1], points[4 * i + 2]));
 }
 
 void tgo_field_evaluate(const tgo_problem* p, const float* points, uint32_t n, float* out)

@@ -25,6 +25,19 @@ enum { TGO_MODEL_SH = 0, TGO_MODEL_DTI = 1 };
 enum { TGO_ALGO_TRANSPORT = 0, TGO_ALGO_DIFFUSION = 1 };
 enum { TGO_RNG_MWC64X = 0, TGO_RNG_PHILOX = 1 };
 
+/* Boundary BVH in the reference's layout (domain.py:72-116, bvh.cl:6-14):
+ * preorder nodes, leaves with left = right = -1 and (first, count) into
+ * ordered_triangles, float32 node bounds, float4 vertices, uint4 triangles. */
+typedef struct {
+    const float* vertices;              /* (V, 4) */
+    const uint32_t* triangles;          /* (T, 4), 4th unused */
+    const float* bounds_min;            /* (N, 4) */
+    const float* bounds_max;            /* (N, 4) */
+    const int32_t* nodes;               /* (N, 4): left, right, first, count */
+    const uint32_t* ordered_triangles;  /* leaf slots -> triangle ids */
+    uint32_t n_nodes;
+} tgo_bvh;
+
 typedef struct {
     /* domain (domain.py:350-356): int32 mask, dims, inverse affine rows */
     const int32_t* mask;
@@ -50,6 +63,10 @@ typedef struct {
     /* output */
     float save_at;
     uint32_t n_steps;
+    /* closed-surface domain; when set, the mask above is not used.  A seed is
+     * inside by tgo_mesh_contains; a streamline stops at the first step whose
+     * segment from the previous point hits the surface (bvh.cl:83-131). */
+    const tgo_bvh* mesh;
 } tgo_problem;
 
 /* tracking.py:93-149: dense (n_seeds, n_steps, 4) points and lengths.
@@ -77,6 +94,24 @@ void tgo_seeds_from_fod(int32_t model, uint32_t n_coefficients, const float* fod
                         const float* voxels, uint32_t nnz, const float affine[16],
                         const uint32_t* states, uint32_t n_seeds, float* seeds,
                         int n_threads);
+
+/* bvh.cl:83-131: closest hit of the segment start-end; returns found and
+ * writes the triangle id, barycentric (1-u-v, u, v) and the segment
+ * parameter t in (1e-6, 1]. */
+int tgo_bvh_segment_hit(const tgo_bvh* b, const float start[3], const float end[3], uint32_t* triangle,
+                        float barycentric[3], float* t);
+
+/* Number of triangles the segment crosses (bvh.cl:16-80 tests, max_t = 1). */
+uint32_t tgo_bvh_count_hits(const tgo_bvh* b, const float start[3], const float end[3]);
+
+/* Inside test of a closed surface: majority over three fixed rays of the
+ * parity of surface crossings; 0 outside the root bounds. */
+int tgo_mesh_contains(const tgo_bvh* b, float x, float y, float z);
+
+/* Batched segment hits: starts/ends (n, 4); found (n); triangle (n);
+ * hit (n, 4) = barycentric xyz and t. */
+void tgo_segment_hits(const tgo_bvh* b, const float* starts, const float* ends, uint32_t n, uint8_t* found,
+                      uint32_t* triangle, float* hit, int n_threads);
 
 /* core.cl:180-245 primitives. */
 void tgo_rng_init(uint32_t seed, uint32_t stream_id, uint32_t state[2]);

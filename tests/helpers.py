@@ -12,8 +12,13 @@ def oracle_case(algorithm, domain, field, *, rng_seed=0, save_at=1.0, n_steps=0,
                 seed_offset=0):
     model = O.MODEL_DTI if isinstance(algorithm.local_model, tg.local.DiffusionTensorImaging) else O.MODEL_SH
     algo = O.ALGO_DIFFUSION if isinstance(algorithm, tg.algorithm.Diffusion) else O.ALGO_TRANSPORT
+    if isinstance(domain, tg.domain.Mesh):
+        # the oracle's own BVH build of the same surface
+        mask = dict(mesh=O.BoundaryBvh.build(domain.vertices, domain.faces))
+    else:
+        mask = dict(mask=domain.values, mask_inv_affine=domain.inverse_affine)
     return O.Case(
-        mask=domain.values, mask_inv_affine=domain.inverse_affine,
+        **mask,
         field=field.values, field_inv_affine=field.inverse_affine,
         model=model, algorithm=algo, step_size=algorithm.step_size, gamma=algorithm.gamma,
         noise_variance=getattr(algorithm, "noise_variance", 0.0),

@@ -68,11 +68,35 @@ def check_against_oracle(jobs, result):
                 assert bits_equal(seq[lo + i], want[i, : want_len[i], :3]), (j, b, i)
 
 
-def test_run_jobs_bit_exact(runtime):
+@pytest.mark.parametrize("tuning", [(0, 8, 4), (0, 0, 0), (2, 31, 2), (0, 24, 16)])
+def test_run_jobs_bit_exact(tuning):
+    runtime = tg.CudaRuntime()
+    runtime.set_tuning(*tuning)
     jobs = make_jobs()
     result = jobs_module.run_jobs_packed(jobs, runtime)
     assert result.steps > 0
     check_against_oracle(jobs, result)
+
+
+@pytest.mark.parametrize("tuning", [(0, 0, 0), (1, 31, 3), (0, 16, 16)])
+def test_single_job_tuning_does_not_change_results(tuning):
+    """tg_tracker_run with any launch shape and tail compaction equals the oracle."""
+    from helpers import small_config0
+
+    field, domain, seeds = small_config0(n_voxels=16, n_seeds=3000, seed=5)
+    alg = tg.algorithm.Diffusion(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.1, gamma=1.0,
+                                 noise_variance=0.2, seed=3)
+    twin = tg.algorithm.Diffusion(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.1, gamma=1.0,
+                                  noise_variance=0.2, seed=3)
+    runtime = tg.CudaRuntime()
+    runtime.set_tuning(*tuning)
+    assert runtime.tuning() == dict(zip(("blocks_per_sm", "compact_lanes", "compact_rounds"), tuning))
+    result = tg.tracking.tractogram(alg, domain, field, seeds, save_at=0.25, maximum_streamline_length=40.0,
+                                    runtime=runtime)
+    want, want_len = oracle_case(alg, domain, field, rng_seed=twin.get_rng_seed(), save_at=0.25,
+                                 n_steps=160).tractogram(seeds, n_threads=8)
+    for i, s in enumerate(result.streamlines):
+        assert bits_equal(s, want[i, : want_len[i], :3]), i
 
 
 def test_run_jobs_with_retry_waves_bit_exact():

@@ -35,6 +35,10 @@ EXPORTS = (
     "tg_field_destroy",
     "tg_domain_create",
     "tg_domain_destroy",
+    "tg_domain_create_mesh",
+    "tg_bvh_build_host",
+    "tg_mesh_info",
+    "tg_mesh_segment_hits",
     "tg_tractogram",
     "tg_tractogram_host",
     "tg_tractogram_noalloc",
@@ -43,6 +47,8 @@ EXPORTS = (
     "tg_tracker_run",
     "tg_tracker_run_jobs",
     "tg_tracker_stats",
+    "tg_tracker_set_tuning",
+    "tg_tracker_get_tuning",
     "tg_tracker_copy_points",
     "tg_seeds_from_fod",
     "tg_domain_contains",
@@ -118,6 +124,11 @@ def load() -> ctypes.CDLL:
         "tg_field_destroy": ([P], ctypes.c_int),
         "tg_domain_create": ([P, U32, U32, U32, P, P, ctypes.POINTER(P)], ctypes.c_int),
         "tg_domain_destroy": ([P], ctypes.c_int),
+        "tg_domain_create_mesh": ([P, U32, P, U32, P, ctypes.POINTER(P)], ctypes.c_int),
+        "tg_bvh_build_host": ([P, U32, P, U32, ctypes.POINTER(U32), ctypes.POINTER(U32), P, P, P, P, P, P],
+                              ctypes.c_int),
+        "tg_mesh_info": ([P, ctypes.POINTER(U32), ctypes.POINTER(U32), P, ctypes.POINTER(U64)], ctypes.c_int),
+        "tg_mesh_segment_hits": ([P, P, P, U32, P, P, P, P], ctypes.c_int),
         "tg_tractogram": ([AP, P, P, P, U32, F, U32, P, P, P], ctypes.c_int),
         "tg_tractogram_host": ([AP, P, P, P, U32, F, U32, P, P, P], ctypes.c_int),
         "tg_tractogram_noalloc": ([AP, P, P, P, U32, U32, P, F, U32, P, P, P], ctypes.c_int),
@@ -128,6 +139,8 @@ def load() -> ctypes.CDLL:
         "tg_tracker_run_jobs": ([P, ctypes.POINTER(Job), U32, ctypes.c_int, P, P, ctypes.POINTER(U64),
                                  ctypes.POINTER(U64), P], ctypes.c_int),
         "tg_tracker_stats": ([P, ctypes.POINTER(F), ctypes.POINTER(U32), ctypes.POINTER(U32)], ctypes.c_int),
+        "tg_tracker_set_tuning": ([P, U32, U32, U32], ctypes.c_int),
+        "tg_tracker_get_tuning": ([P, ctypes.POINTER(U32), ctypes.POINTER(U32), ctypes.POINTER(U32)], ctypes.c_int),
         "tg_tracker_copy_points": ([P, P, U64, U64, ctypes.c_int, P], ctypes.c_int),
         "tg_seeds_from_fod": ([I32, U32, P, P, U32, P, P, U32, P, P], ctypes.c_int),
         "tg_domain_contains": ([P, P, U32, P, P], ctypes.c_int),

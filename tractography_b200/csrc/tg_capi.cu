@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "tg_internal.h"
+#include "tg_step.cuh"
 #include "tractography_b200.h"
 
 using namespace tg;
@@ -62,6 +63,14 @@ struct tg_tracker {
     uint32_t* d_class_lists = nullptr;   // job lists and prefixes of all classes
     size_t cap_class_lists = 0;
     unsigned long long* d_class_counters = nullptr;
+    // launch shape and tail compaction (tg_tracker_set_tuning); slot
+    // kClassKinds holds the single-job tracker's carry buffers
+    uint32_t blocks_per_sm = 0;        // 0: the occupancy maximum
+    uint32_t compact_lanes = 8;        // 0: no compaction
+    uint32_t compact_rounds = 4;
+    LaneCarry* carry[kClassKinds + 1][2] = {};
+    size_t carry_cap[kClassKinds + 1] = {};
+    unsigned int* carry_count = nullptr;   // 2 per slot
     // statistics of the last run
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     float kernel_ms = 0.0f;
@@ -144,13 +153,19 @@ int make_track_params(const tg_algorithm* a, const tg_domain* d, const tg_field*
         return fail(TG_ERR_INVALID_ARGUMENT, "save_at must be finite and positive");
     TrackParams p;
     std::memset(&p, 0, sizeof p);
-    p.dgrid = grid_of(d->d.inv_affine, d->d.nx, d->d.ny, d->d.nz);
-    p.mask = d->d.mask;
+    p.domain_kind = d->d.kind;
     p.fgrid = grid_of(f->d.inv_affine, f->d.nx, f->d.ny, f->d.nz);
     p.field = f->d.data;
     p.cpad = f->d.cpad;
-    p.same_grid = d->d.nx == f->d.nx && d->d.ny == f->d.ny && d->d.nz == f->d.nz &&
-                  std::memcmp(d->d.inv_affine, f->d.inv_affine, 12 * sizeof(float)) == 0;
+    if (d->d.kind == kDomainMesh) {
+        p.mesh = d->d.mesh;
+        p.same_grid = 0;
+    } else {
+        p.dgrid = grid_of(d->d.inv_affine, d->d.nx, d->d.ny, d->d.nz);
+        p.mask = d->d.mask;
+        p.same_grid = d->d.nx == f->d.nx && d->d.ny == f->d.ny && d->d.nz == f->d.nz &&
+                      std::memcmp(d->d.inv_affine, f->d.inv_affine, 12 * sizeof(float)) == 0;
+    }
     p.algorithm = a->algorithm;
     p.algo = algo_params(a);
     p.save_at = save_at;
@@ -294,7 +309,81 @@ int tg_domain_destroy(tg_domain* domain)
 {
     if (domain == nullptr) return TG_OK;
     if (domain->d.mask) cudaFree(domain->d.mask);
+    if (domain->d.nodes) cudaFree(domain->d.nodes);
+    if (domain->d.tris) cudaFree(domain->d.tris);
+    if (domain->d.dist) cudaFree(domain->d.dist);
     delete domain;
+    return TG_OK;
+}
+
+int tg_domain_create_mesh(const double* vertices, uint32_t n_vertices, const uint32_t* faces, uint32_t n_faces,
+                          void* stream, tg_domain** out)
+{
+    if (out == nullptr || vertices == nullptr || faces == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    BoundaryBvhHost b;
+    std::string err;
+    if (build_boundary_bvh(vertices, n_vertices, faces, n_faces, &b, &err) != 0)
+        return fail(TG_ERR_INVALID_ARGUMENT, err);
+    tg_domain* d = new tg_domain();
+    const cudaError_t e = upload_mesh(b, &d->d, as_stream(stream));
+    if (e != cudaSuccess) {
+        tg_domain_destroy(d);
+        return fail_cuda(e, "tg_domain_create_mesh");
+    }
+    *out = d;
+    return TG_OK;
+}
+
+int tg_bvh_build_host(const double* vertices, uint32_t n_vertices, const uint32_t* faces, uint32_t n_faces,
+                      uint32_t* n_triangles, uint32_t* n_nodes, float* vertices4, uint32_t* triangles4,
+                      float* bounds_min, float* bounds_max, int32_t* nodes, uint32_t* ordered_triangles)
+{
+    if (vertices == nullptr || faces == nullptr || n_triangles == nullptr || n_nodes == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    BoundaryBvhHost b;
+    std::string err;
+    if (build_boundary_bvh(vertices, n_vertices, faces, n_faces, &b, &err) != 0)
+        return fail(TG_ERR_INVALID_ARGUMENT, err);
+    *n_triangles = b.n_triangles;
+    *n_nodes = b.n_nodes;
+    if (vertices4 == nullptr || triangles4 == nullptr || bounds_min == nullptr || bounds_max == nullptr ||
+        nodes == nullptr || ordered_triangles == nullptr)
+        return TG_OK;
+    std::memcpy(vertices4, b.vertices4.data(), b.vertices4.size() * sizeof(float));
+    std::memcpy(triangles4, b.triangles4.data(), b.triangles4.size() * sizeof(uint32_t));
+    std::memcpy(bounds_min, b.bounds_min.data(), b.bounds_min.size() * sizeof(float));
+    std::memcpy(bounds_max, b.bounds_max.data(), b.bounds_max.size() * sizeof(float));
+    std::memcpy(nodes, b.nodes.data(), b.nodes.size() * sizeof(int32_t));
+    std::memcpy(ordered_triangles, b.ordered.data(), b.ordered.size() * sizeof(uint32_t));
+    return TG_OK;
+}
+
+int tg_mesh_info(const tg_domain* domain, uint32_t* n_triangles, uint32_t* n_nodes, uint32_t grid[3],
+                 uint64_t* device_bytes)
+{
+    if (domain == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "domain is null");
+    if (domain->d.kind != kDomainMesh) return fail(TG_ERR_INVALID_ARGUMENT, "not a mesh domain");
+    if (n_triangles) *n_triangles = domain->d.n_triangles;
+    if (n_nodes) *n_nodes = domain->d.mesh.n_nodes;
+    if (grid) {
+        grid[0] = domain->d.nx;
+        grid[1] = domain->d.ny;
+        grid[2] = domain->d.nz;
+    }
+    if (device_bytes) *device_bytes = domain->d.bytes;
+    return TG_OK;
+}
+
+int tg_mesh_segment_hits(const tg_domain* domain, const float* starts, const float* ends, uint32_t n,
+                         uint8_t* found, uint32_t* triangle, float* hit, void* stream)
+{
+    if (domain == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "domain is null");
+    if (domain->d.kind != kDomainMesh) return fail(TG_ERR_INVALID_ARGUMENT, "not a mesh domain");
+    if (n == 0) return TG_OK;
+    TG_TRY(launch_mesh_segment_hits(domain->d.mesh, reinterpret_cast<const float4*>(starts),
+                                    reinterpret_cast<const float4*>(ends), n, found, triangle,
+                                    reinterpret_cast<float4*>(hit), as_stream(stream)));
     return TG_OK;
 }
 
@@ -391,7 +480,34 @@ int tg_tracker_destroy(tg_tracker* t)
     cudaFree(t->d_job_base);
     cudaFree(t->d_class_lists);
     cudaFree(t->d_class_counters);
+    for (int k = 0; k <= kClassKinds; ++k) {
+        cudaFree(t->carry[k][0]);
+        cudaFree(t->carry[k][1]);
+    }
+    cudaFree(t->carry_count);
     delete t;
+    return TG_OK;
+}
+
+int tg_tracker_set_tuning(tg_tracker* t, uint32_t blocks_per_sm, uint32_t compact_lanes, uint32_t compact_rounds)
+{
+    if (t == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "tracker is null");
+    if (compact_lanes > 31) return fail(TG_ERR_INVALID_ARGUMENT, "compact_lanes must be at most 31");
+    if (compact_rounds > 16) return fail(TG_ERR_INVALID_ARGUMENT, "compact_rounds must be at most 16");
+    if (blocks_per_sm > 32) return fail(TG_ERR_INVALID_ARGUMENT, "blocks_per_sm must be at most 32");
+    t->blocks_per_sm = blocks_per_sm;
+    t->compact_lanes = compact_lanes;
+    t->compact_rounds = compact_rounds;
+    return TG_OK;
+}
+
+int tg_tracker_get_tuning(const tg_tracker* t, uint32_t* blocks_per_sm, uint32_t* compact_lanes,
+                          uint32_t* compact_rounds)
+{
+    if (t == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "tracker is null");
+    if (blocks_per_sm) *blocks_per_sm = t->blocks_per_sm;
+    if (compact_lanes) *compact_lanes = t->compact_lanes;
+    if (compact_rounds) *compact_rounds = t->compact_rounds;
     return TG_OK;
 }
 
@@ -401,6 +517,24 @@ int tg_tracker_stats(const tg_tracker* t, float* kernel_ms, uint32_t* waves, uin
     if (kernel_ms) *kernel_ms = t->kernel_ms;
     if (waves) *waves = t->waves;
     if (launches) *launches = t->launches;
+    return TG_OK;
+}
+
+// Carry buffers of one slot for a grid of `lanes` threads (each lane hands
+// over at most one streamline per round).
+static int tracker_carry(tg_tracker* t, int slot, size_t lanes)
+{
+    if (t->carry_count == nullptr) {
+        TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->carry_count), 2 * (kClassKinds + 1) * sizeof(unsigned int)));
+    }
+    if (t->carry_cap[slot] >= lanes && t->carry[slot][0] != nullptr) return TG_OK;
+    cudaFree(t->carry[slot][0]);
+    cudaFree(t->carry[slot][1]);
+    t->carry[slot][0] = t->carry[slot][1] = nullptr;
+    t->carry_cap[slot] = 0;
+    TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->carry[slot][0]), lanes * sizeof(LaneCarry)));
+    TG_TRY(cudaMalloc(reinterpret_cast<void**>(&t->carry[slot][1]), lanes * sizeof(LaneCarry)));
+    t->carry_cap[slot] = lanes;
     return TG_OK;
 }
 
@@ -524,7 +658,15 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
     pp.lengths = t->lengths;
 
     const int block = persistent_block_size();
-    const int grid = sm_count() * persistent_blocks_per_sm(field->d, algorithm->algorithm);
+    int per_sm = persistent_blocks_per_sm(field->d, algorithm->algorithm, domain->d.kind);
+    if (t->blocks_per_sm > 0 && (int)t->blocks_per_sm < per_sm) per_sm = (int)t->blocks_per_sm;
+    const int grid = sm_count() * per_sm;
+    const uint32_t rounds = t->compact_lanes > 0 ? t->compact_rounds : 0u;
+    if (rounds > 0) {
+        st = tracker_carry(t, kClassKinds, (size_t)grid * block);
+        if (st != TG_OK) return st;
+    }
+    unsigned int* ccount = t->carry_count + 2 * kClassKinds;
 
     t->h_len.resize(n_seeds);
     TG_TRY(cudaMemsetAsync(t->counters + 1, 0, sizeof(unsigned long long), s));
@@ -541,10 +683,21 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
         pp.pool = t->pool;
         pp.chunk_next = t->chunk_next;
         pp.n_chunks = t->n_chunks;
-        TG_TRY(cudaMemsetAsync(t->counters, 0, sizeof(unsigned long long), s));
         TG_TRY(cudaMemsetAsync(t->chunk_counter, 0, sizeof(unsigned int), s));
         TG_TRY(cudaEventRecord(t->ev_start, s));
-        TG_TRY(launch_track_persistent(field->d, pp, grid, block, s));
+        // round 0 pulls seeds; rounds 1..R resume the streamlines handed over
+        // by sparse warps of the previous round; the last round compacts no more
+        for (uint32_t r = 0; r <= rounds; ++r) {
+            TG_TRY(cudaMemsetAsync(t->counters, 0, sizeof(unsigned long long), s));
+            pp.carry_in = r == 0 ? nullptr : t->carry[kClassKinds][(r - 1) & 1];
+            pp.carry_in_count = r == 0 ? nullptr : ccount + ((r - 1) & 1);
+            pp.carry_out = r < rounds ? t->carry[kClassKinds][r & 1] : nullptr;
+            pp.carry_out_count = ccount + (r & 1);
+            pp.compact_lanes = t->compact_lanes;
+            if (r < rounds) TG_TRY(cudaMemsetAsync(ccount + (r & 1), 0, sizeof(unsigned int), s));
+            TG_TRY(launch_track_persistent(field->d, pp, grid, block, s));
+            t->launches += 1;
+        }
         TG_TRY(cudaEventRecord(t->ev_stop, s));
         TG_TRY(cudaMemcpyAsync(t->h_len.data(), t->lengths, (size_t)n_seeds * sizeof(uint32_t),
                                cudaMemcpyDeviceToHost, s));
@@ -553,7 +706,6 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
         TG_TRY(cudaEventElapsedTime(&wave_ms, t->ev_start, t->ev_stop));
         t->kernel_ms += wave_ms;
         t->waves += 1;
-        t->launches += 1;
 
         t->h_done.clear();
         t->h_retry.clear();
@@ -625,6 +777,8 @@ int tg_tracker_run_jobs(tg_tracker* t, const tg_job* jobs, uint32_t n_jobs, int 
         TrackParams tp;
         int st = make_track_params(&J.algorithm, J.domain, J.field, J.save_at, J.n_steps, &tp);
         if (st != TG_OK) return fail(st, "job " + std::to_string(j) + ": " + g_error);
+        if (tp.domain_kind != kDomainImage)
+            return fail(TG_ERR_UNSUPPORTED, "job " + std::to_string(j) + ": mesh domains run through tg_tracker_run");
         if (J.n_steps == 0) return fail(TG_ERR_INVALID_ARGUMENT, "job " + std::to_string(j) + ": n_steps must be positive");
         if (J.n_seeds > 0 && (J.seeds == nullptr || J.batch_rng_seeds == nullptr || J.batch_size == 0))
             return fail(TG_ERR_INVALID_ARGUMENT, "job " + std::to_string(j) + ": missing seeds or batch seeds");
@@ -773,6 +927,19 @@ int tg_tracker_run_jobs(tg_tracker* t, const tg_job* jobs, uint32_t n_jobs, int 
         for (int k = 0; k < kClassKinds; ++k)
             for (uint32_t j : members[k]) budget[k] += (uint64_t)jobs[j].n_seeds * jobs[j].n_steps;
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return budget[a] > budget[b]; });
+        // launch shapes and carry buffers first: no allocation while kernels run
+        const uint32_t rounds = t->compact_lanes > 0 ? t->compact_rounds : 0u;
+        std::vector<int> kgrid(kClassKinds, 0);
+        for (int k : order) {
+            if (members[k].empty()) continue;
+            int per_sm = class_blocks_per_sm(k);
+            if (t->blocks_per_sm > 0 && (int)t->blocks_per_sm < per_sm) per_sm = (int)t->blocks_per_sm;
+            kgrid[k] = sms * per_sm;
+            if (rounds > 0) {
+                st = tracker_carry(t, k, (size_t)kgrid[k] * 128);
+                if (st != TG_OK) return st;
+            }
+        }
         for (int k : order) {
             ClassDev cls;
             std::memset(&cls, 0, sizeof cls);
@@ -789,12 +956,24 @@ int tg_tracker_run_jobs(tg_tracker* t, const tg_job* jobs, uint32_t n_jobs, int 
             }
             if (cls.n_items == 0) continue;
             wave_items += cls.n_items;
-            TG_TRY(cudaStreamWaitEvent(t->class_stream[k], t->ev_fork, 0));
-            TG_TRY(launch_track_class(mp, cls, sms, t->class_stream[k]));
-            TG_TRY(cudaEventRecord(t->class_done[k], t->class_stream[k]));
+            cudaStream_t ks = t->class_stream[k];
+            TG_TRY(cudaStreamWaitEvent(ks, t->ev_fork, 0));
+            unsigned int* ccount = t->carry_count + 2 * k;
+            for (uint32_t r = 0; r <= rounds; ++r) {
+                MultiParams mk = mp;
+                mk.carry_in = r == 0 ? nullptr : t->carry[k][(r - 1) & 1];
+                mk.carry_in_count = r == 0 ? nullptr : ccount + ((r - 1) & 1);
+                mk.carry_out = r < rounds ? t->carry[k][r & 1] : nullptr;
+                mk.carry_out_count = ccount + (r & 1);
+                mk.compact_lanes = t->compact_lanes;
+                if (r > 0) TG_TRY(cudaMemsetAsync(cls.counter, 0, sizeof(unsigned long long), ks));
+                if (r < rounds) TG_TRY(cudaMemsetAsync(ccount + (r & 1), 0, sizeof(unsigned int), ks));
+                TG_TRY(launch_track_class(mk, cls, kgrid[k], ks));
+                t->launches += 1;
+            }
+            TG_TRY(cudaEventRecord(t->class_done[k], ks));
             TG_TRY(cudaStreamWaitEvent(s, t->class_done[k], 0));
             launched.push_back(k);
-            t->launches += 1;
         }
         TG_TRY(cudaEventRecord(t->ev_stop, s));
         TG_TRY(cudaMemcpyAsync(t->h_len.data(), t->lengths, n_total * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
@@ -886,6 +1065,11 @@ int tg_domain_contains(const tg_domain* domain, const float* points, uint32_t n,
 {
     if (domain == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "domain is null");
     if (n == 0) return TG_OK;
+    if (domain->d.kind == kDomainMesh) {
+        TG_TRY(launch_mesh_contains(domain->d.mesh, reinterpret_cast<const float4*>(points), n, out,
+                                    as_stream(stream)));
+        return TG_OK;
+    }
     TG_TRY(launch_contains(domain->d, reinterpret_cast<const float4*>(points), n, out, as_stream(stream)));
     return TG_OK;
 }

@@ -8,9 +8,15 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <string>
+#include <vector>
+
+#include "tg_bvh.cuh"
 #include "tg_device.cuh"
 
 namespace tg {
+
+struct LaneCarry;   // tg_step.cuh
 
 constexpr int kChunkPoints = 32;   // points per output chunk (chunk = 32 x 12 B)
 
@@ -28,17 +34,27 @@ struct FieldDev {
     size_t bytes = 0;
 };
 
-// Device-resident image domain (domain.py:267-398): uint8 mask, same voxel
-// order as the reference's int32 mask.
+// Device-resident domain.  Image (domain.py:267-398): uint8 mask, same voxel
+// order as the reference's int32 mask.  Mesh: a closed triangle surface with
+// its boundary BVH (domain.py:44-116) and distance grid (tg_bvh.cuh).
 struct DomainDev {
+    int kind = kDomainImage;
     uint8_t* mask = nullptr;
     uint32_t nx = 0, ny = 0, nz = 0;
     float inv_affine[16];
     size_t bytes = 0;
+    // mesh
+    float4* nodes = nullptr;
+    float4* tris = nullptr;
+    uint8_t* dist = nullptr;
+    uint32_t n_triangles = 0;
+    MeshDev mesh{};
 };
 
 // Everything one tracking launch needs, by value.
 struct TrackParams {
+    int domain_kind;         // kDomainImage (mask) or kDomainMesh
+    MeshDev mesh;
     Grid dgrid;
     const uint8_t* mask;
     Grid fgrid;
@@ -75,6 +91,16 @@ struct PersistentParams {
     int32_t* first_chunk;         // n_seeds
     uint32_t* lengths;            // n_seeds; kOverflowBit set when retried
     unsigned long long* steps_done;   // total accepted steps
+    // Tail compaction.  A round pulls seeds (carry_in null) or resumes the
+    // streamlines carry_in[0 .. *carry_in_count) left by the previous round;
+    // with carry_out set, a warp whose queue is empty and whose live lanes
+    // number at most compact_lanes writes them to carry_out and exits, so
+    // the next round runs them in full warps.
+    const LaneCarry* carry_in;
+    const unsigned int* carry_in_count;
+    LaneCarry* carry_out;
+    unsigned int* carry_out_count;
+    uint32_t compact_lanes;
 };
 
 // Many jobs queued at once (tg_multi.cu).  Job j covers global seed indices
@@ -107,6 +133,12 @@ struct ClassDev {
 };
 
 struct MultiParams {
+    // tail compaction, per class round as in PersistentParams
+    const LaneCarry* carry_in;
+    const unsigned int* carry_in_count;
+    LaneCarry* carry_out;
+    unsigned int* carry_out_count;
+    uint32_t compact_lanes;
     const JobDev* jobs;
     const uint32_t* job_base;   // n_jobs + 1
     uint32_t n_jobs;
@@ -122,8 +154,29 @@ struct MultiParams {
 
 // One persistent launch per class (code path); classes run concurrently on
 // separate streams and share the point pool.
-cudaError_t launch_track_class(const MultiParams& mp, const ClassDev& cls, int sms, cudaStream_t stream);
+cudaError_t launch_track_class(const MultiParams& mp, const ClassDev& cls, int grid, cudaStream_t stream);
+int class_blocks_per_sm(int kind);
 int class_kind(int model, int lmax, int algorithm);
+
+// Closed-surface domain (tg_mesh.cu).  The boundary BVH in the reference's
+// array layout (domain.py:100-116), built on the host.
+struct BoundaryBvhHost {
+    std::vector<float> vertices4;      // (V, 4), w = 1
+    std::vector<uint32_t> triangles4;  // (T, 4), kept (non-degenerate) faces
+    std::vector<float> bounds_min;     // (N, 4)
+    std::vector<float> bounds_max;     // (N, 4)
+    std::vector<int32_t> nodes;        // (N, 4): left, right, first, count
+    std::vector<uint32_t> ordered;     // (T,)
+    uint32_t n_nodes = 0;
+    uint32_t n_triangles = 0;
+};
+int build_boundary_bvh(const double* vertices, uint32_t n_vertices, const uint32_t* faces, uint32_t n_faces,
+                       BoundaryBvhHost* out, std::string* error);
+cudaError_t upload_mesh(const BoundaryBvhHost& b, DomainDev* d, cudaStream_t stream);
+cudaError_t launch_mesh_segment_hits(const MeshDev& m, const float4* starts, const float4* ends, uint32_t n,
+                                     uint8_t* found, uint32_t* triangle, float4* hit, cudaStream_t stream);
+cudaError_t launch_mesh_contains(const MeshDev& m, const float4* points, uint32_t n, uint8_t* out,
+                                 cudaStream_t stream);
 
 // Launchers (tg_track.cu).
 cudaError_t launch_track_dense(const FieldDev& f, const TrackParams& p, const float4* seeds,
@@ -156,7 +209,7 @@ cudaError_t launch_rng_streams(int which, uint32_t s0, uint32_t s1, uint32_t n, 
 
 int lmax_for(uint32_t n_params);
 int persistent_block_size();
-int persistent_blocks_per_sm(const FieldDev& f, int algorithm);
+int persistent_blocks_per_sm(const FieldDev& f, int algorithm, int domain_kind);
 
 }  // namespace tg
 

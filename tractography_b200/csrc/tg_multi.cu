@@ -81,10 +81,17 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
     uint32_t fill = 0;
     uint32_t g = 0;
 
+    const unsigned long long n_items = mp.carry_in != nullptr ? *mp.carry_in_count : cls.n_items;
+
     auto fetch = [&]() -> bool {
         while (true) {
             const unsigned long long k = atomicAdd(cls.counter, 1ull);
-            if (k >= cls.n_items) return false;
+            if (k >= n_items) return false;
+            if (mp.carry_in != nullptr) {
+                lane_restore(s, mp.carry_in[k], g, chunk, fill);
+                J = mp.jobs + (upper_bound_u32(mp.job_base, mp.n_jobs + 1, g) - 1);
+                return true;
+            }
             uint32_t job, i;
             if (cls.item_ids != nullptr) {
                 g = cls.item_ids[k];
@@ -115,7 +122,14 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
     };
 
     bool live = fetch();
-    while (live) {
+    while (true) {
+        const unsigned active = __ballot_sync(0xffffffffu, live);
+        if (active == 0u) break;
+        if (mp.carry_out != nullptr && warp_should_compact(active, mp.compact_lanes)) {
+            if (live) lane_save(mp.carry_out + atomicAdd(mp.carry_out_count, 1u), s, g, chunk, fill);
+            break;
+        }
+        if (!live) continue;
         bool done = s.n >= J->t.n_steps;
         bool overflow = false;
         if (!done) {
@@ -142,43 +156,62 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
 }
 
 template <int MODEL, int LMAX, int ALGO>
-__global__ void __launch_bounds__(128) track_class_kernel(const MultiParams mp, const ClassDev cls)
+__global__ void __launch_bounds__(128, 5) track_class_kernel(const MultiParams mp, const ClassDev cls)
 {
     const unsigned long long steps = drain_class<MODEL, LMAX, ALGO>(mp, cls);
     if (steps != 0) atomicAdd(mp.steps_done, steps);
 }
 
 template <int M, int L, int A>
-cudaError_t launch_class(const MultiParams& mp, const ClassDev& cls, int sms, cudaStream_t stream)
+struct ClassLaunch {
+    static cudaError_t run(const MultiParams& mp, const ClassDev& cls, int grid, cudaStream_t stream)
+    {
+        track_class_kernel<M, L, A><<<grid, 128, 0, stream>>>(mp, cls);
+        return cudaGetLastError();
+    }
+};
+
+template <int M, int L, int A>
+struct ClassOccupancy {
+    static cudaError_t run(int* blocks)
+    {
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, track_class_kernel<M, L, A>, 128, 0);
+    }
+};
+
+template <template <int, int, int> class Fn, typename... Args>
+cudaError_t class_dispatch(int kind, Args&&... args)
 {
-    int blocks = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, track_class_kernel<M, L, A>, 128, 0);
-    if (e != cudaSuccess) return e;
-    const int grid = sms * (blocks > 0 ? blocks : 1);
-    track_class_kernel<M, L, A><<<grid, 128, 0, stream>>>(mp, cls);
-    return cudaGetLastError();
+    switch (kind) {
+    case kSH0T: return Fn<kModelSH, 0, kTransport>::run(args...);
+    case kSH0D: return Fn<kModelSH, 0, kDiffusion>::run(args...);
+    case kSH2T: return Fn<kModelSH, 2, kTransport>::run(args...);
+    case kSH2D: return Fn<kModelSH, 2, kDiffusion>::run(args...);
+    case kSH4T: return Fn<kModelSH, 4, kTransport>::run(args...);
+    case kSH4D: return Fn<kModelSH, 4, kDiffusion>::run(args...);
+    case kSH6T: return Fn<kModelSH, 6, kTransport>::run(args...);
+    case kSH6D: return Fn<kModelSH, 6, kDiffusion>::run(args...);
+    case kSH8T: return Fn<kModelSH, 8, kTransport>::run(args...);
+    case kSH8D: return Fn<kModelSH, 8, kDiffusion>::run(args...);
+    case kDTIT: return Fn<kModelDTI, 0, kTransport>::run(args...);
+    case kDTID: return Fn<kModelDTI, 0, kDiffusion>::run(args...);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace
 
-cudaError_t launch_track_class(const MultiParams& mp, const ClassDev& cls, int sms, cudaStream_t s)
+int class_blocks_per_sm(int kind)
+{
+    int blocks = 0;
+    if (class_dispatch<ClassOccupancy>(kind, &blocks) != cudaSuccess || blocks < 1) blocks = 1;
+    return blocks;
+}
+
+cudaError_t launch_track_class(const MultiParams& mp, const ClassDev& cls, int grid, cudaStream_t s)
 {
     if (cls.n_items == 0) return cudaSuccess;
-    switch (cls.kind) {
-    case kSH0T: return launch_class<kModelSH, 0, kTransport>(mp, cls, sms, s);
-    case kSH0D: return launch_class<kModelSH, 0, kDiffusion>(mp, cls, sms, s);
-    case kSH2T: return launch_class<kModelSH, 2, kTransport>(mp, cls, sms, s);
-    case kSH2D: return launch_class<kModelSH, 2, kDiffusion>(mp, cls, sms, s);
-    case kSH4T: return launch_class<kModelSH, 4, kTransport>(mp, cls, sms, s);
-    case kSH4D: return launch_class<kModelSH, 4, kDiffusion>(mp, cls, sms, s);
-    case kSH6T: return launch_class<kModelSH, 6, kTransport>(mp, cls, sms, s);
-    case kSH6D: return launch_class<kModelSH, 6, kDiffusion>(mp, cls, sms, s);
-    case kSH8T: return launch_class<kModelSH, 8, kTransport>(mp, cls, sms, s);
-    case kSH8D: return launch_class<kModelSH, 8, kDiffusion>(mp, cls, sms, s);
-    case kDTIT: return launch_class<kModelDTI, 0, kTransport>(mp, cls, sms, s);
-    case kDTID: return launch_class<kModelDTI, 0, kDiffusion>(mp, cls, sms, s);
-    default: return cudaErrorInvalidValue;
-    }
+    return class_dispatch<ClassLaunch>(cls.kind, mp, cls, grid, s);
 }
 
 }  // namespace tg

@@ -165,6 +165,7 @@ extern "C" int tg_tractogram_noalloc(const tg_algorithm* algorithm, const tg_dom
     int model = 0, lmax = 0;
     int st = track_params_from_handles(algorithm, domain, field, save_at, n_steps, &p, &model, &lmax);
     if (st != TG_OK) return st;
+    if (p.domain_kind != kDomainImage) return fail(TG_ERR_UNSUPPORTED, "tg_tractogram_noalloc takes image domains");
     if (n_seeds == 0) return TG_OK;
     if (n_steps == 0) return fail(TG_ERR_INVALID_ARGUMENT, "n_steps must be positive");
     if (batch_size == 0) return fail(TG_ERR_INVALID_ARGUMENT, "batch_size must be positive");

@@ -28,33 +28,55 @@ struct Lane {
     float dvx, dvy, dvz;
     float fvx, fvy, fvz;
     uint32_t steps;
+    // closed-surface domain: the point of the last passed domain test
+    float lx, ly, lz;
 };
 
 // One iteration of tracking.py:121-147 after the n < N_STEPS test.
 // Returns 0 when the streamline stops (domain or field check failed),
 // 1 after a step without a saved point, 2 after a step that saved point q.
-template <int MODEL, int LMAX, int ALGO, int CPAD>
+//
+// DOM selects the domain test: the image mask (domain.py:358-382), or a
+// closed surface, where the seed must be inside and every later point must
+// be reached by a segment from the previous one that does not hit the
+// surface (the found flag of bvh.cl:83-131).
+template <int MODEL, int LMAX, int ALGO, int CPAD, int DOM = kDomainImage>
 __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (&c)[CPAD],
                                           float& qx, float& qy, float& qz)
 {
-    // domain.py:358-382 and field.py:88-114 share the voxel-space point when
-    // both images have the same grid (the default of tg.tractogram).
-    const float ax = dot4(p.dgrid.row0, s.px, s.py, s.pz, 1.0f);
-    const float ay = dot4(p.dgrid.row1, s.px, s.py, s.pz, 1.0f);
-    const float az = dot4(p.dgrid.row2, s.px, s.py, s.pz, 1.0f);
-    const float vx = floorf(ax + 0.5f), vy = floorf(ay + 0.5f), vz = floorf(az + 0.5f);
-    if (vx != s.dvx || vy != s.dvy || vz != s.dvz) {
-        if (!(vx >= 0.0f && vx < (float)p.dgrid.nx && vy >= 0.0f && vy < (float)p.dgrid.ny &&
-              vz >= 0.0f && vz < (float)p.dgrid.nz))
+    float ax, ay, az;
+    if constexpr (DOM == kDomainMesh) {
+        if (s.steps == 0u) {
+            if (!mesh_contains(p.mesh, s.px, s.py, s.pz)) return 0;
+        } else if (mesh_segment_blocked(p.mesh, s.lx, s.ly, s.lz, s.px, s.py, s.pz)) {
             return 0;
-        const int64_t k = ((int64_t)(int32_t)vx * p.dgrid.ny + (int32_t)vy) * p.dgrid.nz + (int32_t)vz;
-        if (__ldg(p.mask + k) == 0) return 0;
-        s.dvx = vx;
-        s.dvy = vy;
-        s.dvz = vz;
+        }
+        s.lx = s.px;
+        s.ly = s.py;
+        s.lz = s.pz;
+        ax = dot4(p.fgrid.row0, s.px, s.py, s.pz, 1.0f);
+        ay = dot4(p.fgrid.row1, s.px, s.py, s.pz, 1.0f);
+        az = dot4(p.fgrid.row2, s.px, s.py, s.pz, 1.0f);
+    } else {
+        // domain.py:358-382 and field.py:88-114 share the voxel-space point
+        // when both images have the same grid (the default of tg.tractogram).
+        ax = dot4(p.dgrid.row0, s.px, s.py, s.pz, 1.0f);
+        ay = dot4(p.dgrid.row1, s.px, s.py, s.pz, 1.0f);
+        az = dot4(p.dgrid.row2, s.px, s.py, s.pz, 1.0f);
+        const float vx = floorf(ax + 0.5f), vy = floorf(ay + 0.5f), vz = floorf(az + 0.5f);
+        if (vx != s.dvx || vy != s.dvy || vz != s.dvz) {
+            if (!(vx >= 0.0f && vx < (float)p.dgrid.nx && vy >= 0.0f && vy < (float)p.dgrid.ny &&
+                  vz >= 0.0f && vz < (float)p.dgrid.nz))
+                return 0;
+            const int64_t k = ((int64_t)(int32_t)vx * p.dgrid.ny + (int32_t)vy) * p.dgrid.nz + (int32_t)vz;
+            if (__ldg(p.mask + k) == 0) return 0;
+            s.dvx = vx;
+            s.dvy = vy;
+            s.dvz = vz;
+        }
     }
     float bx = ax, by = ay, bz = az;
-    if (!p.same_grid) {
+    if (DOM == kDomainImage && !p.same_grid) {
         bx = dot4(p.fgrid.row0, s.px, s.py, s.pz, 1.0f);
         by = dot4(p.fgrid.row1, s.px, s.py, s.pz, 1.0f);
         bz = dot4(p.fgrid.row2, s.px, s.py, s.pz, 1.0f);
@@ -97,6 +119,57 @@ __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (
     return 1;
 }
 
+// A live streamline handed from one round of a persistent launch to the
+// next (tail compaction): everything the step reads, plus its output
+// cursor.  The voxel caches are not carried; the next step reloads them,
+// which gives the same values.
+struct __align__(16) LaneCarry {
+    float px, py, pz, time;
+    float ox, oy, oz, lx;
+    float ly, lz;
+    uint32_t n, steps;
+    uint32_t mwc_x, mwc_c, rng_step, item;
+    uint64_t rng_index;
+    int32_t chunk;
+    uint32_t fill;
+};
+
+__device__ __forceinline__ void lane_save(LaneCarry* dst, const Lane& s, uint32_t item, int32_t chunk,
+                                          uint32_t fill)
+{
+    LaneCarry c;
+    c.px = s.px; c.py = s.py; c.pz = s.pz; c.time = s.time;
+    c.ox = s.ox; c.oy = s.oy; c.oz = s.oz; c.lx = s.lx;
+    c.ly = s.ly; c.lz = s.lz; c.n = s.n; c.steps = s.steps;
+    c.mwc_x = s.rng.mwc.x; c.mwc_c = s.rng.mwc.c; c.rng_step = s.rng.step; c.item = item;
+    c.rng_index = s.rng.index;
+    c.chunk = chunk;
+    c.fill = fill;
+    *dst = c;
+}
+
+__device__ __forceinline__ void lane_restore(Lane& s, const LaneCarry& c, uint32_t& item, int32_t& chunk,
+                                             uint32_t& fill)
+{
+    s.px = c.px; s.py = c.py; s.pz = c.pz; s.time = c.time;
+    s.ox = c.ox; s.oy = c.oy; s.oz = c.oz; s.lx = c.lx;
+    s.ly = c.ly; s.lz = c.lz; s.n = c.n; s.steps = c.steps;
+    s.rng.mwc.x = c.mwc_x; s.rng.mwc.c = c.mwc_c; s.rng.step = c.rng_step; item = c.item;
+    s.rng.index = c.rng_index;
+    s.dvx = s.dvy = s.dvz = __int_as_float(0x7fc00000);
+    s.fvx = s.fvy = s.fvz = __int_as_float(0x7fc00000);
+    chunk = c.chunk;
+    fill = c.fill;
+}
+
+// Tail compaction rule, evaluated by whole warps: once a lane of the warp
+// has found its queue empty (so the warp is not full), a warp with at most
+// `compact_lanes` live lanes hands them to the next round and exits.
+__device__ __forceinline__ bool warp_should_compact(unsigned active, uint32_t compact_lanes)
+{
+    return active != 0xffffffffu && (uint32_t)__popc(active) <= compact_lanes;
+}
+
 __device__ __forceinline__ void lane_init(Lane& s, float4 a, float4 b, uint32_t rng_seed,
                                           uint32_t stream_id, uint64_t index)
 {
@@ -110,6 +183,9 @@ __device__ __forceinline__ void lane_init(Lane& s, float4 a, float4 b, uint32_t 
     s.dvx = s.dvy = s.dvz = __int_as_float(0x7fc00000);
     s.fvx = s.fvy = s.fvz = __int_as_float(0x7fc00000);
     s.steps = 0u;
+    s.lx = a.x;
+    s.ly = a.y;
+    s.lz = a.z;
 }
 
 }  // namespace tg

@@ -31,7 +31,7 @@ namespace tg {
 
 // ------------------------------------------------------------------ dense
 
-template <int MODEL, int LMAX, int ALGO>
+template <int MODEL, int LMAX, int ALGO, int DOM>
 __global__ void __launch_bounds__(128) track_dense_kernel(TrackParams p, const float4* __restrict__ seeds,
                                                           uint32_t n_seeds, uint32_t rng_seed,
                                                           uint64_t seed_offset, float4* __restrict__ out,
@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128) track_dense_kernel(TrackParams p, const f
     line[0] = a;
     while (s.n < p.n_steps) {
         float qx, qy, qz;
-        const int r = track_step<MODEL, LMAX, ALGO, CPAD>(p, s, c, qx, qy, qz);
+        const int r = track_step<MODEL, LMAX, ALGO, CPAD, DOM>(p, s, c, qx, qy, qz);
         if (r == 0) break;
         if (r == 2) {
             line[s.n] = make_float4(qx, qy, qz, 1.0f);
@@ -90,7 +90,7 @@ __device__ __forceinline__ bool emit_point(const PersistentParams& pp, int32_t& 
     return true;
 }
 
-template <int MODEL, int LMAX, int ALGO>
+template <int MODEL, int LMAX, int ALGO, int DOM>
 __global__ void __launch_bounds__(128, 5) track_persistent_kernel(const PersistentParams pp)
 {
     constexpr int CPAD = ModelShape<MODEL, LMAX>::CPAD;
@@ -106,11 +106,17 @@ __global__ void __launch_bounds__(128, 5) track_persistent_kernel(const Persiste
     bool live = false;
     unsigned long long steps_total = 0;
 
-    // Pull the next seed; returns false when the queue is drained.
+    const unsigned long long n_items = pp.carry_in != nullptr ? *pp.carry_in_count : pp.n_items;
+
+    // Pull the next seed (or carried streamline); false when the queue is drained.
     auto fetch = [&]() -> bool {
         while (true) {
             const unsigned long long it = atomicAdd(pp.item_counter, 1ull);
-            if (it >= pp.n_items) return false;
+            if (it >= n_items) return false;
+            if (pp.carry_in != nullptr) {
+                lane_restore(s, pp.carry_in[it], item, chunk, fill);
+                return true;
+            }
             item = pp.item_ids != nullptr ? pp.item_ids[it] : (uint32_t)it;
             const float4 a = pp.seeds[2 * (size_t)item];
             const float4 b = pp.seeds[2 * (size_t)item + 1];
@@ -130,12 +136,19 @@ __global__ void __launch_bounds__(128, 5) track_persistent_kernel(const Persiste
     };
 
     live = fetch();
-    while (live) {
+    while (true) {
+        const unsigned active = __ballot_sync(0xffffffffu, live);
+        if (active == 0u) break;
+        if (pp.carry_out != nullptr && warp_should_compact(active, pp.compact_lanes)) {
+            if (live) lane_save(pp.carry_out + atomicAdd(pp.carry_out_count, 1u), s, item, chunk, fill);
+            break;
+        }
+        if (!live) continue;
         bool done = s.n >= p.n_steps;
         bool overflow = false;
         if (!done) {
             float qx, qy, qz;
-            const int r = track_step<MODEL, LMAX, ALGO, CPAD>(p, s, c, qx, qy, qz);
+            const int r = track_step<MODEL, LMAX, ALGO, CPAD, DOM>(p, s, c, qx, qy, qz);
             if (r == 0) {
                 done = true;
             } else if (r == 2) {
@@ -190,11 +203,13 @@ __global__ void __launch_bounds__(256) gather_kernel(const float* __restrict__ p
 
 // --------------------------------------------------------------- dispatch
 
-template <template <int, int, int> class Fn, typename... Args>
-cudaError_t dispatch(int model, int lmax, int algo, Args&&... args)
+template <template <int, int, int, int> class Fn, typename... Args>
+cudaError_t dispatch(int model, int lmax, int algo, int dom, Args&&... args)
 {
-#define TG_CASE(M, L, A) \
-    if (model == M && (M == kModelDTI || lmax == L) && algo == A) return Fn<M, L, A>::run(args...);
+#define TG_CASE(M, L, A)                                                                     \
+    if (model == M && (M == kModelDTI || lmax == L) && algo == A)                            \
+        return dom == kDomainMesh ? Fn<M, L, A, kDomainMesh>::run(args...)                   \
+                                  : Fn<M, L, A, kDomainImage>::run(args...);
     TG_CASE(kModelSH, 0, kTransport) TG_CASE(kModelSH, 0, kDiffusion)
     TG_CASE(kModelSH, 2, kTransport) TG_CASE(kModelSH, 2, kDiffusion)
     TG_CASE(kModelSH, 4, kTransport) TG_CASE(kModelSH, 4, kDiffusion)
@@ -205,32 +220,32 @@ cudaError_t dispatch(int model, int lmax, int algo, Args&&... args)
     return cudaErrorInvalidValue;
 }
 
-template <int M, int L, int A>
+template <int M, int L, int A, int D>
 struct DenseLaunch {
     static cudaError_t run(const TrackParams& p, const float4* seeds, uint32_t n, uint32_t rng_seed,
                            uint64_t seed_offset, float4* out, uint32_t* lengths, cudaStream_t stream)
     {
         const int block = 128;
         const int grid = (int)((n + block - 1) / block);
-        track_dense_kernel<M, L, A><<<grid, block, 0, stream>>>(p, seeds, n, rng_seed, seed_offset, out, lengths);
+        track_dense_kernel<M, L, A, D><<<grid, block, 0, stream>>>(p, seeds, n, rng_seed, seed_offset, out, lengths);
         return cudaGetLastError();
     }
 };
 
-template <int M, int L, int A>
+template <int M, int L, int A, int D>
 struct PersistentLaunch {
     static cudaError_t run(const PersistentParams& p, int grid, int block, cudaStream_t stream)
     {
-        track_persistent_kernel<M, L, A><<<grid, block, 0, stream>>>(p);
+        track_persistent_kernel<M, L, A, D><<<grid, block, 0, stream>>>(p);
         return cudaGetLastError();
     }
 };
 
-template <int M, int L, int A>
+template <int M, int L, int A, int D>
 struct PersistentOccupancy {
     static cudaError_t run(int* blocks)
     {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, track_persistent_kernel<M, L, A>,
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, track_persistent_kernel<M, L, A, D>,
                                                              persistent_block_size(), 0);
     }
 };
@@ -244,10 +259,11 @@ int lmax_for(uint32_t n_params)
 
 int persistent_block_size() { return 128; }
 
-int persistent_blocks_per_sm(const FieldDev& f, int algorithm)
+int persistent_blocks_per_sm(const FieldDev& f, int algorithm, int domain_kind)
 {
     int blocks = 0;
-    if (dispatch<PersistentOccupancy>(f.model, f.lmax, algorithm, &blocks) != cudaSuccess || blocks < 1)
+    if (dispatch<PersistentOccupancy>(f.model, f.lmax, algorithm, domain_kind, &blocks) != cudaSuccess ||
+        blocks < 1)
         blocks = 1;
     return blocks;
 }
@@ -257,7 +273,8 @@ cudaError_t launch_track_dense(const FieldDev& f, const TrackParams& p, const fl
                                uint32_t* lengths, cudaStream_t stream)
 {
     if (n_seeds == 0) return cudaSuccess;
-    return dispatch<DenseLaunch>(f.model, f.lmax, p.algorithm, p, seeds, n_seeds, rng_seed, seed_offset,
+    return dispatch<DenseLaunch>(f.model, f.lmax, p.algorithm, p.domain_kind, p, seeds, n_seeds, rng_seed,
+                                 seed_offset,
                                  out, lengths, stream);
 }
 
@@ -265,7 +282,7 @@ cudaError_t launch_track_persistent(const FieldDev& f, const PersistentParams& p
                                     cudaStream_t stream)
 {
     if (p.n_items == 0) return cudaSuccess;
-    return dispatch<PersistentLaunch>(f.model, f.lmax, p.t.algorithm, p, grid, block, stream);
+    return dispatch<PersistentLaunch>(f.model, f.lmax, p.t.algorithm, p.t.domain_kind, p, grid, block, stream);
 }
 
 cudaError_t launch_gather(const float* pool, const int32_t* chunk_next, const int32_t* first_chunk,

@@ -8,7 +8,13 @@ inside the image and nonzero (domain.py:358-382).  On the GPU the mask is a
 The reference also builds a voxel-face boundary mesh and a BVH in every
 ``Image`` constructor for boundary seeding and connectome end points
 (domain.py:44-116, 219-264); the streamline tracker never reads them, so
-this module does not build them.
+``Image`` does not build them.
+
+``Mesh`` makes a closed triangle surface the domain.  Its BVH is the
+reference's boundary BVH (median split of domain.py:72-116, traversal of
+utils/bvh.cl:83-131), built natively on the host and kept on the device: a
+seed is inside by a three-ray crossing-parity vote, and a streamline stops
+at the first step whose segment from the previous point hits the surface.
 """
 
 from __future__ import annotations
@@ -75,13 +81,124 @@ class Image(BaseDomain):
         return obj.handle
 
 
+class Mesh(BaseDomain):
+    """Domain bounded by a closed, outward-wound triangle surface.
+
+    ``Mesh(vertices, faces)`` with (V, 3) vertices and (F, 3) vertex indices,
+    or ``Mesh(mesh)`` for any object with ``vertices`` and ``faces`` (a
+    trimesh.Trimesh, for example).  Faces of zero or non-finite area are
+    dropped as in domain.py:49-57.
+    """
+
+    def __init__(self, vertices, faces=None):
+        if faces is None:
+            vertices, faces = vertices.vertices, vertices.faces
+        self.vertices = np.ascontiguousarray(vertices, dtype=np.float64)
+        self.faces = np.ascontiguousarray(faces, dtype=np.uint32)
+        if self.vertices.ndim != 2 or self.vertices.shape[1] != 3:
+            raise ValueError("vertices must have shape (n_vertices, 3)")
+        if self.faces.ndim != 2 or self.faces.shape[1] != 3:
+            raise ValueError("faces must have shape (n_faces, 3)")
+        if len(self.faces) == 0:
+            raise ValueError("The boundary mesh must contain at least one triangle.")
+        if self.faces.max() >= len(self.vertices):
+            raise ValueError("face vertex index out of range")
+        self._device = {}
+
+    def bvh_arrays(self) -> dict:
+        """The boundary BVH in the reference's layout (domain.py:100-116).
+
+        Built by the library on the host: ``vertices`` (V, 4) float32,
+        ``triangles`` (T, 4) uint32 of the kept faces, ``bounds_min`` and
+        ``bounds_max`` (N, 4) float32, ``nodes`` (N, 4) int32 (left, right,
+        first, count) and ``ordered_triangles`` (T,) uint32.
+        """
+        lib = _lib.load()
+        nt, nn = ctypes.c_uint32(), ctypes.c_uint32()
+        P = ctypes.c_void_p
+        v, f = self.vertices, self.faces
+        args = (v.ctypes.data_as(P), len(v), f.ctypes.data_as(P), len(f), ctypes.byref(nt), ctypes.byref(nn))
+        _lib.check(lib.tg_bvh_build_host(*args, None, None, None, None, None, None))
+        out = {
+            "vertices": np.empty((len(v), 4), np.float32),
+            "triangles": np.empty((nt.value, 4), np.uint32),
+            "bounds_min": np.empty((nn.value, 4), np.float32),
+            "bounds_max": np.empty((nn.value, 4), np.float32),
+            "nodes": np.empty((nn.value, 4), np.int32),
+            "ordered_triangles": np.empty(nt.value, np.uint32),
+        }
+        _lib.check(lib.tg_bvh_build_host(*args, *(a.ctypes.data_as(P) for a in out.values())))
+        return out
+
+    def contains(self, points) -> np.ndarray:
+        """Inside test on the GPU (three-ray crossing-parity vote)."""
+        return contains(self, points)
+
+    def device(self, runtime):
+        """The ``tg_domain`` of this surface for ``runtime``."""
+        key = id(runtime)
+        obj = self._device.get(key)
+        if obj is None:
+            from .runtime import DeviceObject
+
+            handle = ctypes.c_void_p()
+            with runtime.device_scope():
+                _lib.check(runtime.lib.tg_domain_create_mesh(
+                    self.vertices.ctypes.data_as(ctypes.c_void_p), len(self.vertices),
+                    self.faces.ctypes.data_as(ctypes.c_void_p), len(self.faces),
+                    ctypes.c_void_p(runtime.stream_handle), ctypes.byref(handle)))
+            obj = DeviceObject(handle, runtime.lib.tg_domain_destroy)
+            self._device[key] = obj
+        return obj.handle
+
+    def info(self, runtime=None) -> dict:
+        """Triangles, BVH nodes, distance-grid cells and device bytes."""
+        from .runtime import default_runtime
+
+        runtime = runtime or default_runtime()
+        nt, nn, nbytes = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64()
+        grid = (ctypes.c_uint32 * 3)()
+        _lib.check(runtime.lib.tg_mesh_info(self.device(runtime), ctypes.byref(nt), ctypes.byref(nn), grid,
+                                            ctypes.byref(nbytes)))
+        return {"triangles": nt.value, "nodes": nn.value, "grid": tuple(grid), "device_bytes": nbytes.value}
+
+    def segment_hits(self, starts, ends, runtime=None):
+        """bvh_segment_hit (utils/bvh.cl:83-131) per segment on the GPU.
+
+        Returns (found, triangle index among the kept faces, (n, 4)
+        barycentric coordinates and segment parameter t)."""
+        from .runtime import default_runtime
+
+        import torch
+
+        runtime = runtime or default_runtime()
+        n = len(starts)
+        s4 = np.zeros((n, 4), np.float32)
+        e4 = np.zeros((n, 4), np.float32)
+        s4[:, :3], e4[:, :3] = np.asarray(starts)[:, :3], np.asarray(ends)[:, :3]
+        if n == 0:
+            return np.zeros(0, bool), np.zeros(0, np.uint32), np.zeros((0, 4), np.float32)
+        with runtime.device_scope():
+            handle = self.device(runtime)
+            ds, de = runtime.to_device(s4), runtime.to_device(e4)
+            found = runtime.empty((n,), torch.uint8)
+            tri = runtime.empty((n,), torch.int32)
+            hit = runtime.empty((n, 4), torch.float32)
+            _lib.check(runtime.lib.tg_mesh_segment_hits(
+                handle, ctypes.c_void_p(ds.data_ptr()), ctypes.c_void_p(de.data_ptr()), n,
+                ctypes.c_void_p(found.data_ptr()), ctypes.c_void_p(tri.data_ptr()), ctypes.c_void_p(hit.data_ptr()),
+                ctypes.c_void_p(runtime.stream_handle)))
+            return (found.cpu().numpy().astype(bool), tri.cpu().numpy().view(np.uint32),
+                    hit.cpu().numpy())
+
+
 def contains(domain: BaseDomain, points, runtime=None) -> np.ndarray:
     """GPU membership test (domain.py:433-491)."""
     points = np.asarray(points)
     n = points.shape[0]
     if n == 0:
         return np.array([], dtype=np.bool_)
-    if not isinstance(domain, Image):
+    if not isinstance(domain, (Image, Mesh)):
         raise NotImplementedError(f"{type(domain).__name__} has no compiled CUDA code path")
     from .runtime import default_runtime
 

@@ -69,6 +69,15 @@ class CudaRuntime:
             self._finalizer = weakref.finalize(self, _destroy, self.lib.tg_tracker_destroy, handle)
         return self._tracker
 
+    def set_tuning(self, blocks_per_sm: int = 0, compact_lanes: int = 8, compact_rounds: int = 4) -> None:
+        """Launch shape and tail compaction of the tracker (results do not depend on them)."""
+        _lib.check(self.lib.tg_tracker_set_tuning(self.tracker(), blocks_per_sm, compact_lanes, compact_rounds))
+
+    def tuning(self) -> dict:
+        b, c, r = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _lib.check(self.lib.tg_tracker_get_tuning(self.tracker(), ctypes.byref(b), ctypes.byref(c), ctypes.byref(r)))
+        return {"blocks_per_sm": b.value, "compact_lanes": c.value, "compact_rounds": r.value}
+
     def device_scope(self):
         return _torch().cuda.device(self.device)
 

@@ -288,3 +288,108 @@ def seeds_in_mask(mask_img, n: int, seed: int = 0) -> np.ndarray:
         return seeds_module.from_mask(mask_img, n)
     finally:
         np.random.set_state(state)
+
+
+def geodesic_sphere(frequency: int):
+    """Unit geodesic sphere: each icosahedron face cut into frequency^2
+    triangles, points projected to the sphere.  Shared edge and corner
+    points are generated once, so the surface is closed; faces are wound
+    outward.  Returns (vertices (V, 3) float64, faces (20 f^2, 3) uint32)."""
+    n = int(frequency)
+    if n < 1:
+        raise ValueError("frequency must be >= 1")
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    corners = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t],
+                        [0, -1, -t], [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
+    ico = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4],
+                    [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9],
+                    [4, 9, 5], [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]])
+    points = [c for c in corners]
+    index = {("c", k): k for k in range(12)}
+
+    def vertex(key, position):
+        k = index.get(key)
+        if k is None:
+            k = len(points)
+            index[key] = k
+            points.append(position)
+        return k
+
+    def edge_point(a, b, k):
+        if k == 0:
+            return a
+        if k == n:
+            return b
+        if a > b:
+            a, b, k = b, a, n - k
+        return vertex(("e", a, b, k), corners[a] + (corners[b] - corners[a]) * (k / n))
+
+    faces = []
+    for f, (A, B, C) in enumerate(ico):
+        grid = {}
+        for i in range(n + 1):
+            for j in range(n + 1 - i):
+                if j == 0:
+                    grid[i, j] = edge_point(A, B, i)
+                elif i == 0:
+                    grid[i, j] = edge_point(A, C, j)
+                elif i + j == n:
+                    grid[i, j] = edge_point(B, C, j)
+                else:
+                    p = corners[A] + (corners[B] - corners[A]) * (i / n) + (corners[C] - corners[A]) * (j / n)
+                    grid[i, j] = vertex(("f", f, i, j), p)
+        for i in range(n):
+            for j in range(n - i):
+                faces.append((grid[i, j], grid[i + 1, j], grid[i, j + 1]))
+                if i + j < n - 1:
+                    faces.append((grid[i + 1, j], grid[i + 1, j + 1], grid[i, j + 1]))
+    v = np.asarray(points, dtype=np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    faces = np.asarray(faces, dtype=np.int64)
+    tri = v[faces]
+    normal = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    inward = np.einsum("ij,ij->i", normal, tri.mean(axis=1)) < 0
+    faces[inward] = faces[inward][:, [0, 2, 1]]
+    return v, faces.astype(np.uint32)
+
+
+def config2_surface(shape=(96, 96, 60), voxel_mm: float = 2.0, frequency: int = 158, fill: float = 0.9):
+    """Closed surface of the DTI/mesh workload: a geodesic sphere (20 f^2
+    triangles; f = 158 gives 499 280) with radius r = 1 + 0.1 Y_2^1 + 0.05 Y_4^0
+    (real orthonormal harmonics), scaled per axis so that its extent is
+    `fill` of the volume's and centred in it (world mm, affine diag(voxel))."""
+    v, f = geodesic_sphere(frequency)
+    x, y, z = v.T
+    ct = np.clip(z, -1.0, 1.0)
+    st = np.sqrt(np.maximum(0.0, 1.0 - ct * ct))
+    phi = np.arctan2(y, x)
+    y21 = np.sqrt(15.0 / (4.0 * np.pi)) * st * ct * np.cos(phi)
+    y40 = 3.0 / 16.0 * np.sqrt(1.0 / np.pi) * (35.0 * ct ** 4 - 30.0 * ct ** 2 + 3.0)
+    r = 1.0 + 0.1 * y21 + 0.05 * y40
+    v = v * r[:, None]
+    lo, hi = v.min(axis=0), v.max(axis=0)
+    extent = (np.asarray(shape, dtype=np.float64) - 1.0) * voxel_mm
+    scale = fill * extent / (hi - lo)
+    centre = extent / 2.0
+    v = (v - (lo + hi) / 2.0) * scale + centre
+    return v, f
+
+
+def seeds_inside(contains, bounds_lo, bounds_hi, n: int, seed: int = 0, chunk: int = 1 << 20) -> np.ndarray:
+    """n seeds uniform inside a region given by a vectorised ``contains``
+    over its bounding box (rejection sampling), with uniform orientations."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.asarray(bounds_lo, np.float64), np.asarray(bounds_hi, np.float64)
+    kept = []
+    have = 0
+    while have < n:
+        p = rng.uniform(lo, hi, (chunk, 3))
+        p = p[np.asarray(contains(p), dtype=bool)]
+        kept.append(p)
+        have += len(p)
+    loc = np.concatenate(kept)[:n]
+    o = rng.normal(size=(n, 3))
+    o /= np.linalg.norm(o, axis=1, keepdims=True)
+    out = np.empty((n, 8), np.float32)
+    out[:, :3], out[:, 3], out[:, 4:7], out[:, 7] = loc, 1.0, o, 0.0
+    return out

@@ -23,6 +23,7 @@ from . import _lib
 from .algorithm import BaseAlgorithm, to_struct
 from .domain import BaseDomain
 from .domain import Image as ImageDomain
+from .domain import Mesh as MeshDomain
 from .field import BaseField
 from .field import Image as ImageField
 from .local import model_id
@@ -64,7 +65,7 @@ def _n_steps(save_at: float, maximum_streamline_length: float) -> int:
 
 
 def _handles(algorithm, domain, field, runtime):
-    if not isinstance(domain, ImageDomain):
+    if not isinstance(domain, (ImageDomain, MeshDomain)):
         raise NotImplementedError(f"{type(domain).__name__} has no compiled CUDA code path")
     if not isinstance(field, ImageField):
         raise NotImplementedError(f"{type(field).__name__} has no compiled CUDA code path")
