@@ -77,8 +77,11 @@ def parse_args():
     p.add_argument("--seeds", type=int, default=1000000, help="seeds per step (one tg.tractogram job)")
     p.add_argument("--batch", type=int, default=50000, help="reference batch_size inside a job")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["config1", "mixed", "config2"], default="config1",
-                   help="config1 (default headline), the 64-job mixed workload, or the DTI + mesh workload")
+    p.add_argument("--workload", choices=["config1", "mixed", "config2", "serve"], default="config1",
+                   help="config1 (default headline), the 64-job mixed workload, the DTI + mesh workload, or "
+                        "serving under Poisson load")
+    p.add_argument("--rates", default="5,20,50,100,200", help="serving: arrival rates (requests/s)")
+    p.add_argument("--duration", type=float, default=6.0, help="serving: seconds of arrivals per rate")
     p.add_argument("--jobs", type=int, default=64, help="jobs of the mixed workload")
     return p.parse_args()
 
@@ -719,6 +722,113 @@ def run_config2(args):
     print(json.dumps(line), flush=True)
 
 
+SERVE_WORKLOAD = ("config4 serving: 8 resident SH lmax 8 volumes (64^3, 96x96x60, 128^3, 145x174x145, two "
+                  "each, 2 mm) and 2 resident mesh boundaries (199k-triangle surfaces on the two 96x96x60 volumes); "
+                  "Poisson arrivals; each request picks a volume uniformly, seeds log-U[1k, 2M], 70% Transport / "
+                  "30% Diffusion (noise_variance U[0.05, 0.2]), step 0.2 mm, save_at 1 and maximum length 300 mm "
+                  "(the reference defaults), batches of 50000; server HBM budget 150 GB minus the resident "
+                  "volumes")
+
+
+def setup_serving(runtime, pool_seeds=2_000_000):
+    import tractography_b200 as tg
+    from tractography_b200 import synthetic
+
+    volumes = []
+    shapes = list(synthetic.MIXED_SHAPES) * 2
+    for i, shape in enumerate(shapes):
+        fod, mask = synthetic.bundle_field(shape, lmax=8, seed=100 + i)
+        field = tg.field.Image(fod)
+        if i in (1, 5):
+            v, f = synthetic.config2_surface(shape=shape, frequency=100)
+            domain = tg.domain.Mesh(v, f)
+            seeds = synthetic.seeds_inside(lambda q, d=domain: tg.domain.contains(d, q, runtime), v.min(axis=0),
+                                           v.max(axis=0), pool_seeds, seed=i)
+        else:
+            domain = tg.domain.Image(mask)
+            seeds = synthetic.uniform_seeds(mask, pool_seeds, seed=i)
+        field.device(runtime, 0)
+        domain.device(runtime)
+        volumes.append((field, domain, seeds, field.values.nbytes))
+    return volumes
+
+
+def make_request(volumes, rng):
+    import tractography_b200 as tg
+    from tractography_b200 import jobs as jobs_module
+
+    field, domain, pool, _ = volumes[int(rng.integers(0, len(volumes)))]
+    n = int(np.exp(rng.uniform(np.log(1e3), np.log(2e6))))
+    start = int(rng.integers(0, len(pool) - n + 1))
+    model = tg.local.RealSymmetricSphericalHarmonics(45)
+    if rng.uniform() < 0.7:
+        alg = tg.algorithm.Transport(model, step_size=0.2, gamma=1.0)
+    else:
+        alg = tg.algorithm.Diffusion(model, step_size=0.2, gamma=1.0, noise_variance=float(rng.uniform(0.05, 0.2)),
+                                     seed=int(rng.integers(1 << 31)))
+    return jobs_module.prepare(field, pool[start:start + n], domain, alg, save_at=1.0,
+                               maximum_streamline_length=300.0, batch_size=50000)
+
+
+def run_serve(args):
+    """Config 4: continuous-batching server under Poisson arrivals; p50/p99 latency per rate."""
+    import torch
+
+    import tractography_b200 as tg
+    from tractography_b200.serve import Server
+
+    torch.cuda.set_device(0)
+    runtime = tg.CudaRuntime(0)
+    volumes = setup_serving(runtime)
+    resident = sum(v[3] for v in volumes)
+    rates = [float(r) for r in args.rates.split(",")]
+    sweep = []
+    sampler = ClockSampler(0)
+    with sampler:
+        for rate in rates:
+            rng = np.random.default_rng(int(rate * 1000))
+            n_req = max(5, int(rate * args.duration))
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+            requests = [make_request(volumes, rng) for _ in range(n_req)]
+            server = Server(runtime, hbm_budget_bytes=150e9 - resident, pool_points=256 << 20, epoch_steps=1024,
+                            max_requests=512)
+            latency, seeds_done = [], 0
+            t0 = time.perf_counter()
+            submitted = 0
+            while len(latency) < n_req:
+                now = time.perf_counter() - t0
+                while submitted < n_req and arrivals[submitted] <= now:
+                    server.submit(requests[submitted])
+                    submitted += 1
+                finished = server.poll()
+                for rid in finished:
+                    _, _, lengths, seconds = server.take(rid, points=False)
+                    latency.append(seconds)
+                    seeds_done += len(lengths)
+                if not finished and server.active == 0 and server.pending == 0 and submitted < n_req:
+                    time.sleep(max(0.0, min(0.002, arrivals[submitted] - (time.perf_counter() - t0))))
+            wall = time.perf_counter() - t0
+            st = server.stats()
+            server.close()
+            lat = np.array(latency)
+            sweep.append({"rate_per_s": rate, "requests": n_req, "p50_s": float(np.percentile(lat, 50)),
+                          "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
+                          "steps": st.steps, "epochs": st.epochs, "busy_s": st.busy_seconds, "wall_s": wall,
+                          "steps_per_s": st.steps / max(1e-9, st.busy_seconds),
+                          "streamlines_per_s": seeds_done / max(1e-9, st.busy_seconds),
+                          "offered_seeds_per_s": float(sum(r.n_seeds for r in requests) / arrivals[-1])})
+            print(json.dumps({"rate": rate, **sweep[-1]}), file=sys.stderr, flush=True)
+    best = max(x["steps_per_s"] for x in sweep)
+    line = {"metric": METRIC, "value": best, "unit": UNIT, "n_gpus": 1, "steps": len(rates), "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator; no dataset)", "workload": "serve",
+            "config": {"workload": SERVE_WORKLOAD, "rates_per_s": rates, "arrival_seconds": args.duration,
+                       "epoch_steps": 1024, "latency": "submission to completion on the device (all streamlines "
+                                                       "harvested into the request's result buffer)"},
+            "sweep": sweep, "clocks": sampler.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -727,6 +837,8 @@ def main():
         run_mixed(args)
     elif args.workload == "config2":
         run_config2(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

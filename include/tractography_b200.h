@@ -208,11 +208,48 @@ int tg_tracker_stats(const tg_tracker* tracker, float* kernel_ms, uint32_t* wave
  * them to the next round and exits; compact_rounds further rounds run those
  * streamlines in full warps, the last round to completion (compact_lanes 0:
  * one launch, no compaction).  Results do not depend on these settings.
- * Defaults: 0, 8, 4.  No reference counterpart: the autotuner's knobs. */
+ * Defaults: 0, 0, 4 (compaction off: a carried streamline waits for the
+ * previous round's tail, which costs more than the sparse warps it saves on
+ * the workloads measured).  No reference counterpart: the autotuner's knobs. */
 int tg_tracker_set_tuning(tg_tracker* tracker, uint32_t blocks_per_sm, uint32_t compact_lanes,
                           uint32_t compact_rounds);
 int tg_tracker_get_tuning(const tg_tracker* tracker, uint32_t* blocks_per_sm, uint32_t* compact_lanes,
                           uint32_t* compact_rounds);
+
+/* Continuous-batching server.  No reference counterpart (the reference
+ * tracks one tg.tractogram call at a time).  Fields, domains and surfaces
+ * stay resident as ordinary handles; requests (tg_job with HOST seeds and
+ * batch seeds, copied at submission) are admitted in arrival order while a
+ * request slot is free and the server's memory -- the shared point pool,
+ * per-request buffers and unclaimed results -- fits in hbm_budget_bytes.
+ * Each tg_server_poll runs one epoch: one persistent launch per code path
+ * on concurrent streams, every lane executing at most epoch_steps loop
+ * iterations; live streamlines carry over to the next epoch and new
+ * arrivals enter the queues between epochs.  After each epoch the
+ * streamlines that finished move from the shared pool to their request's
+ * result buffer.  Finished requests are reported by id; their results equal
+ * the same job run alone.
+ * pool_points sizes the shared point pool (0 = 32M points). */
+typedef struct tg_server tg_server;
+int tg_server_create(uint64_t hbm_budget_bytes, uint64_t pool_points, uint32_t epoch_steps,
+                     uint32_t max_requests, tg_server** out);
+int tg_server_destroy(tg_server* server);
+int tg_server_submit(tg_server* server, const tg_job* job, uint64_t* request_id);
+/* One epoch; writes up to `capacity` finished request ids.  n_active and
+ * n_pending (nullable) report admitted and waiting requests afterwards. */
+int tg_server_poll(tg_server* server, uint64_t* finished_ids, uint32_t capacity, uint32_t* n_finished,
+                   uint32_t* n_active, uint32_t* n_pending);
+/* Size of a finished request's result and seconds from submission to completion. */
+int tg_server_result_size(tg_server* server, uint64_t request_id, uint32_t* n_seeds, uint64_t* n_points,
+                          double* seconds);
+/* Copy the result to host arrays and release it: lengths (n_seeds uint32),
+ * offsets (n_seeds uint64: first point of each streamline in `points`) and
+ * points ((n_points, 3) float32, streamlines in the order they finished).
+ * Any pointer may be null to skip that array. */
+int tg_server_take(tg_server* server, uint64_t request_id, uint32_t* lengths, uint64_t* offsets,
+                   float* points);
+int tg_server_stats(const tg_server* server, uint64_t* steps, uint64_t* epochs, double* busy_seconds,
+                    uint64_t* reserved_bytes);
 
 /* Copy points [first, first + count) of the packed (total_points, 3)
  * float32 buffer of the last run to `dst` (host when dst_on_host != 0). */

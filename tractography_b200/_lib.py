@@ -50,6 +50,13 @@ EXPORTS = (
     "tg_tracker_set_tuning",
     "tg_tracker_get_tuning",
     "tg_tracker_copy_points",
+    "tg_server_create",
+    "tg_server_destroy",
+    "tg_server_submit",
+    "tg_server_poll",
+    "tg_server_result_size",
+    "tg_server_take",
+    "tg_server_stats",
     "tg_seeds_from_fod",
     "tg_domain_contains",
     "tg_field_evaluate",
@@ -142,6 +149,15 @@ def load() -> ctypes.CDLL:
         "tg_tracker_set_tuning": ([P, U32, U32, U32], ctypes.c_int),
         "tg_tracker_get_tuning": ([P, ctypes.POINTER(U32), ctypes.POINTER(U32), ctypes.POINTER(U32)], ctypes.c_int),
         "tg_tracker_copy_points": ([P, P, U64, U64, ctypes.c_int, P], ctypes.c_int),
+        "tg_server_create": ([U64, U64, U32, U32, ctypes.POINTER(P)], ctypes.c_int),
+        "tg_server_destroy": ([P], ctypes.c_int),
+        "tg_server_submit": ([P, ctypes.POINTER(Job), ctypes.POINTER(U64)], ctypes.c_int),
+        "tg_server_poll": ([P, P, U32, ctypes.POINTER(U32), ctypes.POINTER(U32), ctypes.POINTER(U32)], ctypes.c_int),
+        "tg_server_result_size": ([P, U64, ctypes.POINTER(U32), ctypes.POINTER(U64), ctypes.POINTER(ctypes.c_double)],
+                                  ctypes.c_int),
+        "tg_server_take": ([P, U64, P, P, P], ctypes.c_int),
+        "tg_server_stats": ([P, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(ctypes.c_double),
+                             ctypes.POINTER(U64)], ctypes.c_int),
         "tg_seeds_from_fod": ([I32, U32, P, P, U32, P, P, U32, P, P], ctypes.c_int),
         "tg_domain_contains": ([P, P, U32, P, P], ctypes.c_int),
         "tg_field_evaluate": ([P, P, U32, P, P], ctypes.c_int),

@@ -66,7 +66,7 @@ struct tg_tracker {
     // launch shape and tail compaction (tg_tracker_set_tuning); slot
     // kClassKinds holds the single-job tracker's carry buffers
     uint32_t blocks_per_sm = 0;        // 0: the occupancy maximum
-    uint32_t compact_lanes = 8;        // 0: no compaction
+    uint32_t compact_lanes = 0;        // 0: no compaction (measured faster by default)
     uint32_t compact_rounds = 4;
     LaneCarry* carry[kClassKinds + 1][2] = {};
     size_t carry_cap[kClassKinds + 1] = {};

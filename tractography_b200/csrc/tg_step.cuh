@@ -132,12 +132,14 @@ struct __align__(16) LaneCarry {
     uint64_t rng_index;
     int32_t chunk;
     uint32_t fill;
+    uint32_t job;            // job slot (multi-request serving); 0 otherwise
 };
 
 __device__ __forceinline__ void lane_save(LaneCarry* dst, const Lane& s, uint32_t item, int32_t chunk,
-                                          uint32_t fill)
+                                          uint32_t fill, uint32_t job = 0u)
 {
     LaneCarry c;
+    c.job = job;
     c.px = s.px; c.py = s.py; c.pz = s.pz; c.time = s.time;
     c.ox = s.ox; c.oy = s.oy; c.oz = s.oz; c.lx = s.lx;
     c.ly = s.ly; c.lz = s.lz; c.n = s.n; c.steps = s.steps;

@@ -69,7 +69,7 @@ class CudaRuntime:
             self._finalizer = weakref.finalize(self, _destroy, self.lib.tg_tracker_destroy, handle)
         return self._tracker
 
-    def set_tuning(self, blocks_per_sm: int = 0, compact_lanes: int = 8, compact_rounds: int = 4) -> None:
+    def set_tuning(self, blocks_per_sm: int = 0, compact_lanes: int = 0, compact_rounds: int = 4) -> None:
         """Launch shape and tail compaction of the tracker (results do not depend on them)."""
         _lib.check(self.lib.tg_tracker_set_tuning(self.tracker(), blocks_per_sm, compact_lanes, compact_rounds))
 
