@@ -784,8 +784,12 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
     for (uint32_t slot : order) {
         ServeRequest* r = S->slots[slot];
         const int k = r->kind;
+        // an epoch cannot take more seeds than its lanes can start: at most
+        // one per lane per loop iteration
+        const uint64_t cap = std::min<uint64_t>(0x7fffffffull, (uint64_t)S->sms * kind_blocks(S, k) * 128 *
+                                                                   S->epoch_steps);
         for (auto& seg : r->queue) {
-            if (n_new[k] + seg.second > 0x7fffffffull) break;    // offered next epoch
+            if (n_new[k] >= cap) break;                          // offered next epoch
             if (seg_prefix[k].empty()) seg_prefix[k].push_back(0);
             seg_slot[k].push_back(slot);
             seg_start[k].push_back(seg.first);
