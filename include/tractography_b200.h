@@ -296,6 +296,14 @@ int tg_domain_contains(const tg_domain* domain, const float* points, uint32_t n,
                        void* stream);
 /* field.evaluate, field.py:144-197: out (n, C) */
 int tg_field_evaluate(const tg_field* field, const float* points, uint32_t n, float* out, void* stream);
+/* domain.seed, domain.py:494-575 with domain_sample_boundary (:95-120):
+ * n_seeds seeds uniform over a boundary surface's area, pointing inward,
+ * seed i drawing from rng_init(rng_seed, i).  Device arrays: vertices
+ * (n_vertices, 4) float32, triangles (n_triangles, 4) uint32, normalised
+ * cumulative areas (n_triangles) float32 (last = 1); seeds (n_seeds, 8). */
+int tg_boundary_seeds(const float* vertices, uint32_t n_vertices, const uint32_t* triangles,
+                      const float* cumulative_areas, uint32_t n_triangles, uint32_t rng_seed, uint32_t n_seeds,
+                      float* seeds, void* stream);
 /* local.evaluate, local.py:285-363: out (n, 3) = value, d/dtheta, (d/dphi)/sin(theta) */
 int tg_local_evaluate(int32_t model, uint32_t n_parameters, const float* parameters,
                       const float* orientations, uint32_t n, float* out, void* stream);

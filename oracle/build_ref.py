@@ -13,8 +13,9 @@ becomes a run-time value, and one counter increment is inserted before the
 orientation update so accepted steps can be counted.  oracle/clshim.hpp
 supplies the OpenCL built-ins.  g++ compiles each variant in its own
 translation unit and namespace; the outputs go only to oracle/_ref/.
-The boundary BVH traversal (utils/bvh.cl) is compiled the same way with a
-batch driver, for the BVH hit parity tests.
+The boundary BVH traversal (utils/bvh.cl) and the boundary sampler of
+domain.seed are compiled the same way with batch drivers, for the BVH hit
+and boundary-seeding parity tests.
 
 Nothing from the reference is copied into this repository: the sources are
 read from the reference tree at build time.
@@ -226,6 +227,36 @@ extern "C" void tgref_bvh_hits(const float* vertices, const unsigned int* triang
 """
 
 
+SEED_DRIVER = """
+extern "C" void tgref_boundary_seeds(const float* vertices, const unsigned int* triangles, const float* cumulative,
+        unsigned int n_triangles, unsigned int rng_seed, unsigned int n, float* locations, float* orientations)
+{
+    const float4 dummy4[4] = {make_float4(0.0f), make_float4(0.0f), make_float4(0.0f), make_float4(0.0f)};
+    const int4 dummyi4 = make_int4(0);
+    const unsigned int dummyu = 0;
+    const int mask = 1;
+    for (unsigned int g = 0; g < n; ++g) {
+        tgref_global_id = g;
+        seedref::sample_domain_boundary((const float4*)vertices, (const uint4*)triangles, cumulative, n_triangles,
+            dummy4, dummy4, &dummyi4, &dummyu, 0u, &mask, make_uint3(1u, 1u, 1u), dummy4, rng_seed, n,
+            (float4*)locations, (float4*)orientations);
+    }
+}
+"""
+
+
+def capture_seed(ref):
+    """The boundary sampler kernel the reference assembles in domain.seed (domain.py:494-575)."""
+    Image = sys.modules["nibabel.nifti1"].Nifti1Image
+    domain = ref.domain.Image(Image(np.ones((2, 2, 2), np.uint8), np.eye(4)))
+    rt = RecordingRuntime()
+    try:
+        ref.domain.seed(domain, 4, rng_seed=1, runtime=rt)
+    except _Captured:
+        return rt.source
+    raise RuntimeError("the reference did not build a program")
+
+
 def bvh_source(kernel_dir):
     """utils/bvh.cl (the boundary BVH traversal) as C++ with a batch driver."""
     text = rewrite_literals(inline_includes((kernel_dir / "utils" / "bvh.cl").read_text(), kernel_dir))
@@ -266,6 +297,10 @@ def main():
     bpath = OUT / "tgref_bvh.cpp"
     bpath.write_text(bvh_source(kernel_dir))
     sources.append(bpath)
+    spath = OUT / "tgref_seed.cpp"
+    spath.write_text(to_cpp(capture_seed(ref), kernel_dir, "seedref").replace(
+        "extern unsigned int tgref_n_steps;", "") + SEED_DRIVER)
+    sources.append(spath)
     flags = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-march=x86-64-v3",
              "-mtune=generic", "-w", f"-I{HERE}"]
     procs = []

@@ -85,6 +85,7 @@ def lib():
         _lib.tgo_philox.argtypes = [P, P, P]
         _lib.tgo_math.argtypes = [ctypes.c_int, P, U32, P]
         _lib.tgo_segment_hits.argtypes = [P, P, P, U32, P, P, P, ctypes.c_int]
+        _lib.tgo_boundary_seeds.argtypes = [P, P, P, U32, U32, U32, P]
         _lib.tgo_mesh_contains.argtypes = [P, F, F, F]
         _lib.tgo_mesh_contains.restype = ctypes.c_int
         _lib.tgo_bvh_count_hits.argtypes = [P, P, P]
@@ -313,3 +314,13 @@ class BoundaryBvh:
         pts = np.asarray(points, np.float32).reshape(-1, 3)
         f = lib().tgo_mesh_contains
         return np.array([f(ctypes.byref(self.struct), *map(float, q)) for q in pts], dtype=bool)
+
+
+def boundary_seeds(vertices4, triangles4, cumulative, rng_seed, n):
+    """domain.seed (domain.py:494-575): (n, 8) seeds on a boundary surface."""
+    v = np.ascontiguousarray(vertices4, dtype=np.float32)
+    t = np.ascontiguousarray(triangles4, dtype=np.uint32)
+    c = np.ascontiguousarray(cumulative, dtype=np.float32)
+    out = np.zeros((n, 8), np.float32)
+    lib().tgo_boundary_seeds(_ptr(v), _ptr(t), _ptr(c), len(c), rng_seed & 0xFFFFFFFF, n, _ptr(out))
+    return out

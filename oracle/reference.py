@@ -111,3 +111,18 @@ def bvh_hits(vertices4, triangles4, bounds_min, bounds_max, nodes, ordered, star
     fn(*[a.ctypes.data for a in arrays], len(arrays[4]), s4.ctypes.data, e4.ctypes.data, n, found.ctypes.data,
        tri.ctypes.data, hit.ctypes.data)
     return found.astype(bool), tri, hit
+
+
+def boundary_seeds(vertices4, triangles4, cumulative, rng_seed, n):
+    """The reference's boundary sampler (domain.py:95-120 via domain.seed): (n, 8) seeds."""
+    v = np.ascontiguousarray(vertices4, np.float32)
+    t = np.ascontiguousarray(triangles4, np.uint32)
+    c = np.ascontiguousarray(cumulative, np.float32)
+    loc = np.zeros((n, 4), np.float32)
+    ori = np.zeros((n, 4), np.float32)
+    fn = lib().tgref_boundary_seeds
+    P = ctypes.c_void_p
+    fn.argtypes = [P, P, P, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, P, P]
+    fn(v.ctypes.data, t.ctypes.data, c.ctypes.data, len(c), rng_seed & 0xFFFFFFFF, n, loc.ctypes.data,
+       ori.ctypes.data)
+    return np.hstack((loc, ori))

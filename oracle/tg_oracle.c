@@ -552,6 +552,45 @@ void tgo_segment_hits(const tgo_bvh* b, const float* starts, const float* ends, 
     }
 }
 
+/* domain.py:95-120 domain_sample_boundary, once per seed (:520-545). */
+void tgo_boundary_seeds(const float* vertices, const uint32_t* triangles, const float* cumulative,
+                        uint32_t n_triangles, uint32_t rng_seed, uint32_t n, float* seeds)
+{
+    for (uint32_t gid = 0; gid < n; ++gid) {
+        uint32_t st[2];
+        tgo_rng_init(rng_seed, gid, st);
+        const float target = randu(st);
+        uint32_t lower = 0, upper = n_triangles;
+        while (lower < upper) {
+            const uint32_t middle = lower + (upper - lower) / 2;
+            if (cumulative[middle] <= target) lower = middle + 1;
+            else upper = middle;
+        }
+        const uint32_t tri = lower < n_triangles - 1 ? lower : n_triangles - 1;
+        const float* a = vertices + 4 * (size_t)triangles[4 * (size_t)tri];
+        const float* b = vertices + 4 * (size_t)triangles[4 * (size_t)tri + 1];
+        const float* c = vertices + 4 * (size_t)triangles[4 * (size_t)tri + 2];
+        const float root_u = sqrtf(randu(st));
+        const float v = randu(st);
+        float p[3], e1[3], e2[3], nrm[3];
+        for (int k = 0; k < 3; ++k) {
+            p[k] = ((1.0f - root_u) * a[k] + (root_u * (1.0f - v)) * b[k]) + (root_u * v) * c[k];
+            e1[k] = b[k] - a[k];
+            e2[k] = c[k] - a[k];
+        }
+        cross3(e1, e2, nrm);
+        const float len = sqrtf(dot3(nrm, nrm));
+        float* out = seeds + 8 * (size_t)gid;
+        for (int k = 0; k < 3; ++k) {
+            const float o = -(nrm[k] / len);
+            out[k] = p[k] + 1e-4f * o;
+            out[4 + k] = o;
+        }
+        out[3] = 1.0f;
+        out[7] = 0.0f;
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* Tracking loop: tracking.py:105-148                                  */
 /* ------------------------------------------------------------------ */

@@ -113,6 +113,11 @@ int tgo_mesh_contains(const tgo_bvh* b, float x, float y, float z);
 void tgo_segment_hits(const tgo_bvh* b, const float* starts, const float* ends, uint32_t n, uint8_t* found,
                       uint32_t* triangle, float* hit, int n_threads);
 
+/* domain.py:494-575 + domain_sample_boundary (:95-120): seeds (n, 8)
+ * uniform over a boundary surface's area, seed i from rng_init(rng_seed, i). */
+void tgo_boundary_seeds(const float* vertices, const uint32_t* triangles, const float* cumulative,
+                        uint32_t n_triangles, uint32_t rng_seed, uint32_t n, float* seeds);
+
 /* core.cl:180-245 primitives. */
 void tgo_rng_init(uint32_t seed, uint32_t stream_id, uint32_t state[2]);
 void tgo_randu_stream(uint32_t s0, uint32_t s1, uint32_t n, float* out);

@@ -21,7 +21,8 @@ default argsort, which is not stable (introsort, or a SIMD sort on CPUs
 with AVX-512), so on those meshes its tree depends on the machine; they pin
 traversal results, the soup pins the tree.
 
-For each: the reference's BVH arrays (BaseDomain._set_boundary_data,
+For each: the reference's BVH arrays and normalised cumulative triangle
+areas (BaseDomain._set_boundary_data,
 domain.py:44-116, run on the reference's own Python code), and for a set of
 seeded segments (near-surface steps, long chords, axis-parallel and
 zero-length segments) the output of the reference's bvh_segment_hit
@@ -119,6 +120,7 @@ def main() -> None:
         }
         for key, a in arrays.items():
             out[f"{name}_{key}"] = np.asarray(a)
+        out[f"{name}_cumulative"] = np.asarray(h.boundary_cumulative_areas)
         s, e = segments(rng, vv, ff, scale)
         found, tri, hit = R.bvh_hits(*arrays.values(), s, e)
         out[f"{name}_starts"], out[f"{name}_ends"] = s, e

@@ -146,3 +146,34 @@ def test_oracle_mesh_tracking_stops_at_the_surface():
     before = pts[np.arange(4), n[:4] - 2, 0]
     assert np.all(last > 9.95) and np.all(last <= 10.0 + 0.05)
     assert np.all(before <= 10.0) and np.all(last - before > 0.049)
+
+
+def test_voxel_boundary_mesh_matches_reference():
+    """domain.py:219-264 restated: same vertices (float64) and faces."""
+    img = tg.Nifti1Image(G["voxels_mask"].astype(np.uint8), G["voxels_affine"])
+    v, f = tg.domain.Image(img).boundary_mesh()
+    assert np.array_equal(v, G["voxels_input_vertices"])
+    assert np.array_equal(f, G["voxels_input_faces"])
+
+
+@pytest.mark.parametrize("name", ["sphere", "voxels"])
+def test_boundary_arrays_match_reference(name):
+    """domain.py:44-70: kept faces, float32 vertices and cumulative areas bit for bit."""
+    if name == "voxels":
+        dom = tg.domain.Image(tg.Nifti1Image(G["voxels_mask"].astype(np.uint8), G["voxels_affine"]))
+    else:
+        dom = tg.domain.Mesh(G["sphere_input_vertices"], G["sphere_input_faces"])
+    v4, f4, cum = dom.boundary_arrays()
+    assert _same(v4, G[f"{name}_vertices"]) and _same(f4, G[f"{name}_triangles"])
+    assert _same(cum, G[f"{name}_cumulative"])
+
+
+def test_oracle_boundary_seeds_are_on_the_surface_pointing_inward():
+    v, f = synthetic.geodesic_sphere(12)
+    dom = tg.domain.Mesh(v * 10.0, f)
+    s = O.boundary_seeds(*dom.boundary_arrays(), 99, 5000)
+    r = np.linalg.norm(s[:, :3].astype(np.float64), axis=1)
+    assert np.all(r < 10.0) and np.all(r > 9.9)               # on the faceted surface, 1e-4 inside
+    assert np.all(np.einsum("ij,ij->i", s[:, 4:7], s[:, :3]) < 0)   # inward
+    assert np.allclose(np.linalg.norm(s[:, 4:7], axis=1), 1.0, atol=1e-6)
+    assert np.all(s[:, 3] == 1.0) and np.all(s[:, 7] == 0.0)

@@ -131,3 +131,27 @@ def test_tg_tractogram_with_mesh_domain(runtime):
         assert bits_equal(s, want[i, : want_len[i], :3]), i
     info = mesh.info(runtime)
     assert info["triangles"] == len(mesh.faces) and info["nodes"] > 0 and min(info["grid"]) >= 5
+
+
+@pytest.mark.parametrize("kind", ["image", "mesh"])
+def test_boundary_seeds_bit_exact(runtime, kind):
+    """domain.seed on the GPU equals the oracle (pinned to the reference's sampler)."""
+    if kind == "image":
+        fod, mask = synthetic.config0(n=16)
+        dom = tg.domain.Image(mask)
+    else:
+        v, f = synthetic.config2_surface(shape=(24, 24, 16), frequency=20)
+        dom = tg.domain.Mesh(v, f)
+    for rng_seed in (0, 7, 0xFFFFFFFF):
+        got = tg.domain.seed(dom, 20000, rng_seed=rng_seed, runtime=runtime)
+        want = O.boundary_seeds(*dom.boundary_arrays(), rng_seed, 20000)
+        assert bits_equal(got, want)
+
+
+def test_tractogram_with_integer_seeds(runtime):
+    fod, mask = synthetic.config0(n=16)
+    alg = tg.algorithm.Transport(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.2)
+    t = tg.tractogram(fod, 300, mask, alg, save_at=0.25, maximum_streamline_length=20.0, runtime=runtime)
+    assert len(t.streamlines) == 300
+    starts = np.array([s[0] for s in t.streamlines])
+    assert np.all(tg.domain.Image(mask).contains(starts))

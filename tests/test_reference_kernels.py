@@ -114,3 +114,16 @@ def test_config0_transport_single_step_and_length_distribution():
     ends_got = got[np.arange(len(seeds)), got_len - 1, :3]
     for axis in range(3):
         assert ks_2samp(ends_ref[:, axis], ends_got[:, axis]).pvalue > 0.01
+
+
+@pytest.mark.parametrize("name", ["sphere", "voxels"])
+def test_boundary_seeds_match_reference_kernel(name):
+    """domain.seed's sampler: the oracle equals the reference kernel bit for bit."""
+    from pathlib import Path
+
+    G = np.load(Path(__file__).resolve().parent / "golden" / "bvh_reference.npz")
+    args = (G[f"{name}_vertices"], G[f"{name}_triangles"], G[f"{name}_cumulative"])
+    for rng_seed in (0, 12345, 0xFFFFFFFF):
+        want = R.boundary_seeds(*args, rng_seed, 3000)
+        got = O.boundary_seeds(*args, rng_seed, 3000)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

@@ -60,6 +60,7 @@ EXPORTS = (
     "tg_seeds_from_fod",
     "tg_domain_contains",
     "tg_field_evaluate",
+    "tg_boundary_seeds",
     "tg_local_evaluate",
     "tg_update_orientation",
     "tg_rng_stream",
@@ -161,6 +162,7 @@ def load() -> ctypes.CDLL:
         "tg_seeds_from_fod": ([I32, U32, P, P, U32, P, P, U32, P, P], ctypes.c_int),
         "tg_domain_contains": ([P, P, U32, P, P], ctypes.c_int),
         "tg_field_evaluate": ([P, P, U32, P, P], ctypes.c_int),
+        "tg_boundary_seeds": ([P, U32, P, P, U32, U32, U32, P, P], ctypes.c_int),
         "tg_local_evaluate": ([I32, U32, P, P, U32, P, P], ctypes.c_int),
         "tg_update_orientation": ([I32, U32, AP, P, P, U32, P, P], ctypes.c_int),
         "tg_rng_stream": ([I32, U32, U32, U32, U32, P, P], ctypes.c_int),

@@ -323,6 +323,53 @@ cudaError_t launch_update_orientation(int model, uint32_t n_params, int algorith
     return cudaGetLastError();
 }
 
+// domain.py:95-120 domain_sample_boundary + :520-545 per seed: triangle by
+// the normalised cumulative areas, uniform point in it, inward normal, point
+// moved 1e-4 inward.  Vector operations in the reference's order (OpenCL
+// float3 arithmetic component by component, normalize = v / length(v)).
+__global__ void __launch_bounds__(128) boundary_seeds_kernel(const float4* __restrict__ vertices,
+                                                             const uint4* __restrict__ triangles,
+                                                             const float* __restrict__ cumulative,
+                                                             uint32_t n_triangles, uint32_t rng_seed, uint32_t n,
+                                                             float4* __restrict__ out)
+{
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= n) return;
+    Mwc st = rng_init(rng_seed, gid);
+    const float target = randu(st);
+    uint32_t lo = 0, hi = n_triangles;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (cumulative[mid] <= target) lo = mid + 1;
+        else hi = mid;
+    }
+    const uint4 ix = triangles[lo < n_triangles - 1 ? lo : n_triangles - 1];
+    const float4 a = vertices[ix.x], b = vertices[ix.y], c = vertices[ix.z];
+    const float root_u = sqrtf(randu(st));
+    const float v = randu(st);
+    const float wa = 1.0f - root_u, wb = root_u * (1.0f - v), wc = root_u * v;
+    const float sx = (wa * a.x + wb * b.x) + wc * c.x;
+    const float sy = (wa * a.y + wb * b.y) + wc * c.y;
+    const float sz = (wa * a.z + wb * b.z) + wc * c.z;
+    const float e1x = b.x - a.x, e1y = b.y - a.y, e1z = b.z - a.z;
+    const float e2x = c.x - a.x, e2y = c.y - a.y, e2z = c.z - a.z;
+    const float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+    const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+    const float ox = -(nx / len), oy = -(ny / len), oz = -(nz / len);
+    out[2 * (size_t)gid] = make_float4(sx + 1e-4f * ox, sy + 1e-4f * oy, sz + 1e-4f * oz, 1.0f);
+    out[2 * (size_t)gid + 1] = make_float4(ox, oy, oz, 0.0f);
+}
+
+cudaError_t launch_boundary_seeds(const float4* vertices, const uint4* triangles, const float* cumulative,
+                                  uint32_t n_triangles, uint32_t rng_seed, uint32_t n, float4* out,
+                                  cudaStream_t stream)
+{
+    if (n == 0) return cudaSuccess;
+    boundary_seeds_kernel<<<(n + 127) / 128, 128, 0, stream>>>(vertices, triangles, cumulative, n_triangles,
+                                                              rng_seed, n, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_rng_streams(int which, uint32_t s0, uint32_t s1, uint32_t n, uint32_t max, void* out,
                                cudaStream_t stream)
 {

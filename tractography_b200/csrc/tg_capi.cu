@@ -1074,6 +1074,21 @@ int tg_domain_contains(const tg_domain* domain, const float* points, uint32_t n,
     return TG_OK;
 }
 
+int tg_boundary_seeds(const float* vertices, uint32_t n_vertices, const uint32_t* triangles,
+                      const float* cumulative_areas, uint32_t n_triangles, uint32_t rng_seed, uint32_t n_seeds,
+                      float* seeds, void* stream)
+{
+    if (n_seeds == 0) return TG_OK;
+    if (vertices == nullptr || triangles == nullptr || cumulative_areas == nullptr || seeds == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    if (n_triangles == 0 || n_vertices == 0)
+        return fail(TG_ERR_INVALID_ARGUMENT, "The boundary mesh must contain at least one triangle.");
+    TG_TRY(launch_boundary_seeds(reinterpret_cast<const float4*>(vertices), reinterpret_cast<const uint4*>(triangles),
+                                 cumulative_areas, n_triangles, rng_seed, n_seeds, reinterpret_cast<float4*>(seeds),
+                                 as_stream(stream)));
+    return TG_OK;
+}
+
 int tg_field_evaluate(const tg_field* field, const float* points, uint32_t n, float* out, void* stream)
 {
     if (field == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "field is null");

@@ -158,6 +158,11 @@ cudaError_t launch_track_class(const MultiParams& mp, const ClassDev& cls, int g
 int class_blocks_per_sm(int kind);
 int class_kind(int model, int lmax, int algorithm);
 
+// Boundary seeding (tg_aux.cu).
+cudaError_t launch_boundary_seeds(const float4* vertices, const uint4* triangles, const float* cumulative,
+                                  uint32_t n_triangles, uint32_t rng_seed, uint32_t n, float4* out,
+                                  cudaStream_t stream);
+
 // Closed-surface domain (tg_mesh.cu).  The boundary BVH in the reference's
 // array layout (domain.py:100-116), built on the host.
 struct BoundaryBvhHost {

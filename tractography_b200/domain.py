@@ -8,7 +8,7 @@ inside the image and nonzero (domain.py:358-382).  On the GPU the mask is a
 The reference also builds a voxel-face boundary mesh and a BVH in every
 ``Image`` constructor for boundary seeding and connectome end points
 (domain.py:44-116, 219-264); the streamline tracker never reads them, so
-``Image`` does not build them.
+``Image`` builds its boundary only when ``seed`` needs it.
 
 ``Mesh`` makes a closed triangle surface the domain.  Its BVH is the
 reference's boundary BVH (median split of domain.py:72-116, traversal of
@@ -35,6 +35,76 @@ class BaseDomain(ABC):
     def contains(self, points) -> np.ndarray:
         """Authoritative membership test for (n, 3) world-space points."""
 
+    def boundary_mesh(self):
+        """(vertices (V, 3) float64, faces (F, 3)) of the domain's boundary surface."""
+        raise NotImplementedError(f"{type(self).__name__} has no boundary surface")
+
+    def boundary_arrays(self):
+        """The boundary sampler's arrays (domain.py:44-70): float32 vertices
+        (V, 4), uint32 kept faces (T, 4) and float32 normalised cumulative
+        areas (T,), faces of zero or non-finite area dropped."""
+        cached = getattr(self, "_boundary_arrays", None)
+        if cached is not None:
+            return cached
+        vertices, faces = self.boundary_mesh()
+        vertices = np.asarray(vertices, dtype=np.float64)
+        faces = np.asarray(faces, dtype=np.uint32)
+        if len(faces) == 0:
+            raise ValueError("The boundary mesh must contain at least one triangle.")
+        t = vertices[faces]
+        area = 0.5 * np.linalg.norm(np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]), axis=1)
+        valid = np.isfinite(area) & (area > 0)
+        faces, area = faces[valid], area[valid]
+        if len(faces) == 0:
+            raise ValueError("The boundary mesh must contain a non-degenerate triangle.")
+        v4 = np.ones((len(vertices), 4), np.float32)
+        v4[:, :3] = vertices
+        f4 = np.zeros((len(faces), 4), np.uint32)
+        f4[:, :3] = faces
+        total = float(np.sum(area, dtype=np.float64))
+        if not np.isfinite(total) or total <= 0:
+            raise ValueError("The boundary mesh must have a finite, positive area.")
+        cumulative = np.cumsum(area / total).astype(np.float32)
+        cumulative[-1] = 1.0
+        self._boundary_arrays = (v4, f4, cumulative)
+        return self._boundary_arrays
+
+
+def voxel_boundary_mesh(mask, affine):
+    """Surface of the union of the occupied voxel cells (domain.py:219-264).
+
+    Voxel centres have integer coordinates and each voxel occupies a unit
+    cell; a square face (two triangles) is emitted where an occupied voxel
+    meets an empty one or the outside of the array, wound outward (reversed
+    when the affine reflects).  Vertices are the distinct cell corners in
+    lexicographic order of their voxel coordinates."""
+    mask = np.asarray(mask, dtype=bool)
+    # (direction, corner offsets in doubled voxel units), outward winding
+    sides = (
+        ((-1, 0, 0), ((-1, -1, -1), (-1, -1, 1), (-1, 1, 1), (-1, 1, -1))),
+        ((1, 0, 0), ((1, -1, -1), (1, 1, -1), (1, 1, 1), (1, -1, 1))),
+        ((0, -1, 0), ((-1, -1, -1), (1, -1, -1), (1, -1, 1), (-1, -1, 1))),
+        ((0, 1, 0), ((-1, 1, -1), (-1, 1, 1), (1, 1, 1), (1, 1, -1))),
+        ((0, 0, -1), ((-1, -1, -1), (-1, 1, -1), (1, 1, -1), (1, -1, -1))),
+        ((0, 0, 1), ((-1, -1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1))),
+    )
+    padded = np.pad(mask, 1, mode="constant", constant_values=False)
+    quads = []
+    for step, corners in sides:
+        neighbour = padded[tuple(slice(1 + d, 1 + d + n) for d, n in zip(step, mask.shape))]
+        exposed = np.argwhere(mask & ~neighbour)
+        if len(exposed):
+            quads.append(2 * exposed[:, None, :] + np.asarray(corners, dtype=np.int64))
+    doubled = np.concatenate(quads, axis=0).reshape(-1, 3)
+    corners, index = np.unique(doubled, axis=0, return_inverse=True)
+    q = index.reshape(-1, 4)
+    faces = np.concatenate((q[:, (0, 1, 2)], q[:, (0, 2, 3)]), axis=0)
+    affine = np.asarray(affine, dtype=np.float64)
+    vertices = apply_affine(affine, corners.astype(np.float64) * 0.5)
+    if np.linalg.det(affine[:3, :3]) < 0:
+        faces = faces[:, [0, 2, 1]]
+    return vertices, faces
+
 
 class Image(BaseDomain):
     """Domain of the nonzero voxels of a 3D image (domain.py:267-430)."""
@@ -50,6 +120,14 @@ class Image(BaseDomain):
         if not np.any(self.values):
             raise ValueError("Image domain must contain at least one nonzero voxel.")
         self._device = {}
+
+    def boundary_mesh(self):
+        """The voxel-face surface of the mask (domain.py:219-264), built on first use."""
+        cached = getattr(self, "_boundary_mesh", None)
+        if cached is None:
+            cached = voxel_boundary_mesh(self.values != 0, self.affine)
+            self._boundary_mesh = cached
+        return cached
 
     def contains(self, points) -> np.ndarray:
         """NumPy reference of domain.py:400-430."""
@@ -104,6 +182,9 @@ class Mesh(BaseDomain):
         if self.faces.max() >= len(self.vertices):
             raise ValueError("face vertex index out of range")
         self._device = {}
+
+    def boundary_mesh(self):
+        return self.vertices, self.faces
 
     def bvh_arrays(self) -> dict:
         """The boundary BVH in the reference's layout (domain.py:100-116).
@@ -219,12 +300,30 @@ def contains(domain: BaseDomain, points, runtime=None) -> np.ndarray:
 
 
 def seed(domain: BaseDomain, n_seeds: int, rng_seed=None, runtime=None) -> np.ndarray:
-    """Boundary seeding (domain.py:494-575) is not provided by this backend."""
+    """Seeds uniform over the boundary surface area, pointing inward (domain.py:494-575).
+
+    Seed i draws from the MWC64X stream rng_init(rng_seed, i): a uniform
+    target selects the triangle through the normalised cumulative areas, two
+    more give a uniform point in it; the orientation is the inward normal
+    and the point sits 1e-4 along it.  Returns (n_seeds, 8) float32 rows."""
     if not isinstance(n_seeds, (int, np.integer)) or n_seeds < 0:
         raise ValueError("n_seeds must be a non-negative integer.")
     if n_seeds == 0:
         return np.empty((0, 8), dtype=np.float32)
-    raise NotImplementedError(
-        "boundary seeding is not implemented by the CUDA backend; pass an (n_seeds, 8) seed array "
-        "(for example from seeds.from_fod or seeds.from_mask)"
-    )
+    if rng_seed is None:
+        rng_seed = int(np.random.default_rng().integers(0, 2**32, dtype=np.uint32))
+    rng_seed = int(rng_seed) % 2**32
+    v4, f4, cumulative = domain.boundary_arrays()
+    from .runtime import default_runtime
+
+    runtime = runtime or default_runtime()
+    import torch
+
+    with runtime.device_scope():
+        dv, df, dc = runtime.to_device(v4), runtime.to_device(f4), runtime.to_device(cumulative)
+        out = runtime.empty((int(n_seeds), 8), torch.float32)
+        _lib.check(runtime.lib.tg_boundary_seeds(
+            ctypes.c_void_p(dv.data_ptr()), len(v4), ctypes.c_void_p(df.data_ptr()),
+            ctypes.c_void_p(dc.data_ptr()), len(f4), rng_seed, int(n_seeds), ctypes.c_void_p(out.data_ptr()),
+            ctypes.c_void_p(runtime.stream_handle)))
+        return out.cpu().numpy()
