@@ -296,6 +296,18 @@ int tg_domain_contains(const tg_domain* domain, const float* points, uint32_t n,
                        void* stream);
 /* field.evaluate, field.py:144-197: out (n, C) */
 int tg_field_evaluate(const tg_field* field, const float* points, uint32_t n, float* out, void* stream);
+/* tracking.tod (tracking.py:181-385): n_seeds boundary seeds (sampler
+ * arrays as for tg_boundary_seeds, rng_init(algorithm->rng_seed, i) then the
+ * Diffusion noise of the same stream) integrated for at most n_steps
+ * iterations; the lmax-8 real SH basis of the orientation at every iteration
+ * is added into `coefficients`, a device (out_dims[0], out_dims[1],
+ * out_dims[2], 45) float32 array (not cleared; the caller zeroes it), at the
+ * voxel floor(A^-1 p + 0.5) of the output grid (out_inverse_affine,
+ * row-major 4x4).  Additions from different threads are unordered. */
+int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field, const float* vertices,
+           uint32_t n_vertices, const uint32_t* triangles, const float* cumulative_areas, uint32_t n_triangles,
+           uint32_t n_seeds, uint32_t n_steps, const uint32_t out_dims[3], const float out_inverse_affine[16],
+           float* coefficients, void* stream);
 /* domain.seed, domain.py:494-575 with domain_sample_boundary (:95-120):
  * n_seeds seeds uniform over a boundary surface's area, pointing inward,
  * seed i drawing from rng_init(rng_seed, i).  Device arrays: vertices

@@ -86,6 +86,7 @@ def lib():
         _lib.tgo_math.argtypes = [ctypes.c_int, P, U32, P]
         _lib.tgo_segment_hits.argtypes = [P, P, P, U32, P, P, P, ctypes.c_int]
         _lib.tgo_boundary_seeds.argtypes = [P, P, P, U32, U32, U32, P]
+        _lib.tgo_tod.argtypes = [P, P, P, P, U32, U32, U32, P, P, P]
         _lib.tgo_mesh_contains.argtypes = [P, F, F, F]
         _lib.tgo_mesh_contains.restype = ctypes.c_int
         _lib.tgo_bvh_count_hits.argtypes = [P, P, P]
@@ -139,6 +140,16 @@ class Case:
         if return_steps:
             return out, lengths, int(steps)
         return out, lengths
+
+    def tod(self, boundary, n_seeds, n_steps, out_shape, out_inverse_affine):
+        """tracking.py:181-385 raw (un-normalised) TOD coefficients (X, Y, Z, 45)."""
+        v, t, c = (np.ascontiguousarray(a, dt) for a, dt in zip(boundary, (np.float32, np.uint32, np.float32)))
+        dims = np.ascontiguousarray(out_shape, dtype=np.uint32)
+        inv = np.ascontiguousarray(out_inverse_affine, dtype=np.float32)
+        out = np.zeros(tuple(int(x) for x in out_shape) + (45,), np.float32)
+        lib().tgo_tod(ctypes.byref(self.p), _ptr(v), _ptr(t), _ptr(c), len(c), n_seeds, n_steps, _ptr(dims),
+                      _ptr(inv), _ptr(out))
+        return out
 
     def contains(self, points):
         pts = _points4(points)

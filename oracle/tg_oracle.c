@@ -553,12 +553,10 @@ void tgo_segment_hits(const tgo_bvh* b, const float* starts, const float* ends, 
 }
 
 /* domain.py:95-120 domain_sample_boundary, once per seed (:520-545). */
-void tgo_boundary_seeds(const float* vertices, const uint32_t* triangles, const float* cumulative,
-                        uint32_t n_triangles, uint32_t rng_seed, uint32_t n, float* seeds)
+static void sample_boundary(const float* vertices, const uint32_t* triangles, const float* cumulative,
+                            uint32_t n_triangles, uint32_t st[2], float* out)
 {
-    for (uint32_t gid = 0; gid < n; ++gid) {
-        uint32_t st[2];
-        tgo_rng_init(rng_seed, gid, st);
+    {
         const float target = randu(st);
         uint32_t lower = 0, upper = n_triangles;
         while (lower < upper) {
@@ -580,7 +578,6 @@ void tgo_boundary_seeds(const float* vertices, const uint32_t* triangles, const 
         }
         cross3(e1, e2, nrm);
         const float len = sqrtf(dot3(nrm, nrm));
-        float* out = seeds + 8 * (size_t)gid;
         for (int k = 0; k < 3; ++k) {
             const float o = -(nrm[k] / len);
             out[k] = p[k] + 1e-4f * o;
@@ -588,6 +585,16 @@ void tgo_boundary_seeds(const float* vertices, const uint32_t* triangles, const 
         }
         out[3] = 1.0f;
         out[7] = 0.0f;
+    }
+}
+
+void tgo_boundary_seeds(const float* vertices, const uint32_t* triangles, const float* cumulative,
+                        uint32_t n_triangles, uint32_t rng_seed, uint32_t n, float* seeds)
+{
+    for (uint32_t gid = 0; gid < n; ++gid) {
+        uint32_t st[2];
+        tgo_rng_init(rng_seed, gid, st);
+        sample_boundary(vertices, triangles, cumulative, n_triangles, st, seeds + 8 * (size_t)gid);
     }
 }
 
@@ -648,6 +655,84 @@ static uint32_t track_one(const tgo_problem* p, const float* seed, uint32_t gid,
         }
     }
     return n;
+}
+
+static void sh_basis(int lmax, frame_t f, float* Y);
+
+static void tod_flush(float* coefficients, const float* acc, const int32_t* idx, const uint32_t* dims)
+{
+    const size_t base = (((size_t)idx[0] * dims[1] + (size_t)idx[1]) * dims[2] + (size_t)idx[2]) * 45;
+    for (int k = 0; k < 45; ++k) coefficients[base + k] += acc[k];
+}
+
+void tgo_tod(const tgo_problem* p, const float* vertices, const uint32_t* triangles, const float* cumulative,
+             uint32_t n_triangles, uint32_t n_seeds, uint32_t n_steps, const uint32_t out_dims[3],
+             const float out_inverse_affine[16], float* coefficients)
+{
+    const uint32_t C = p->field_dims[3];
+    for (uint32_t gid = 0; gid < n_seeds; ++gid) {
+        rng_t rng;
+        float seed[8];
+        tgo_rng_init(p->rng_seed, gid, rng.mwc);
+        sample_boundary(vertices, triangles, cumulative, n_triangles, rng.mwc, seed);
+        rng.index = p->seed_offset + gid;
+        rng.step = 0u;
+        float pos[3] = {seed[0], seed[1], seed[2]};
+        float o[3] = {seed[4], seed[5], seed[6]};
+        float last[3] = {pos[0], pos[1], pos[2]};
+        int first = 1;
+        float acc[45];
+        int32_t prev[3] = {-1, -1, -1};
+        for (uint32_t step = 0; step < n_steps; ++step) {
+            if (p->mesh) {
+                if (first) {
+                    if (!tgo_mesh_contains(p->mesh, pos[0], pos[1], pos[2])) break;
+                } else {
+                    uint32_t tri;
+                    float bc[3], t;
+                    if (tgo_bvh_segment_hit(p->mesh, last, pos, &tri, bc, &t)) break;
+                }
+                first = 0;
+                last[0] = pos[0];
+                last[1] = pos[1];
+                last[2] = pos[2];
+            } else if (!domain_contains(p, pos[0], pos[1], pos[2])) {
+                break;
+            }
+            const float* c = field_voxel(p, pos[0], pos[1], pos[2]);
+            if (!c) break;
+            int32_t idx[3];
+            int inside = 1;
+            for (int i = 0; i < 3; ++i) {
+                const float v = floorf(dot4(out_inverse_affine + 4 * i, pos[0], pos[1], pos[2], 1.0f) + 0.5f);
+                if (!(v >= 0.0f && v < (float)out_dims[i])) inside = 0;
+                idx[i] = inside ? (int32_t)v : 0;
+            }
+            if (inside) {
+                float Y[45];
+                sh_basis(8, frame_of(o[0], o[1], o[2]), Y);
+                if (idx[0] == prev[0] && idx[1] == prev[1] && idx[2] == prev[2]) {
+                    for (int k = 0; k < 45; ++k) acc[k] += Y[k];
+                } else {
+                    if (prev[0] >= 0) tod_flush(coefficients, acc, prev, out_dims);
+                    for (int k = 0; k < 45; ++k) acc[k] = Y[k];
+                    prev[0] = idx[0];
+                    prev[1] = idx[1];
+                    prev[2] = idx[2];
+                }
+            } else if (prev[0] >= 0) {
+                tod_flush(coefficients, acc, prev, out_dims);
+                prev[0] = prev[1] = prev[2] = -1;
+            }
+            update_orientation(p, c, C, o, &rng);
+            const float len = sqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+            if (!(isfinite(o[0]) && isfinite(o[1]) && isfinite(o[2])) || len < 0.5f) break;
+            pos[0] = fmaf(p->step_size, o[0], pos[0]);
+            pos[1] = fmaf(p->step_size, o[1], pos[1]);
+            pos[2] = fmaf(p->step_size, o[2], pos[2]);
+        }
+        if (prev[0] >= 0) tod_flush(coefficients, acc, prev, out_dims);
+    }
 }
 
 uint64_t tgo_tractogram(const tgo_problem* p, const float* seeds, uint32_t n_seeds,

@@ -118,6 +118,14 @@ void tgo_segment_hits(const tgo_bvh* b, const float* starts, const float* ends, 
 void tgo_boundary_seeds(const float* vertices, const uint32_t* triangles, const float* cumulative,
                         uint32_t n_triangles, uint32_t rng_seed, uint32_t n, float* seeds);
 
+/* tracking.py:181-385 (tod): boundary seeds integrated for at most n_steps
+ * iterations, the lmax-8 SH basis of the orientation added at the output
+ * voxel of every iteration, seeds processed in order; coefficients
+ * (nx, ny, nz, 45) accumulate (not cleared). */
+void tgo_tod(const tgo_problem* p, const float* vertices, const uint32_t* triangles, const float* cumulative,
+             uint32_t n_triangles, uint32_t n_seeds, uint32_t n_steps, const uint32_t out_dims[3],
+             const float out_inverse_affine[16], float* coefficients);
+
 /* core.cl:180-245 primitives. */
 void tgo_rng_init(uint32_t seed, uint32_t stream_id, uint32_t state[2]);
 void tgo_randu_stream(uint32_t s0, uint32_t s1, uint32_t n, float* out);

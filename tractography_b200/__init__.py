@@ -12,7 +12,7 @@ sm_100a CUDA kernels behind the C ABI of ``include/tractography_b200.h``.
 from __future__ import annotations
 
 from . import algorithm as algorithm_module
-from . import core, jobs, local, nifti, streamlines, tracking
+from . import core, jobs, local, nifti, streamlines, tracking, utils
 from . import domain as domain_module
 from . import field as field_module
 from . import seeds
@@ -29,8 +29,80 @@ seeds_module = seeds
 __all__ = [
     "ArraySequence", "BufferAccess", "CudaRuntime", "Nifti1Image", "OpenCLRuntime", "Tractogram",
     "algorithm", "core", "domain", "field", "jobs", "load_tck", "local", "nifti", "save_tck", "seeds",
-    "streamlines", "tracking", "tractogram",
+    "streamlines", "tod", "tracking", "tractogram", "utils",
 ]
+
+
+def tod(field, n_seeds: int = 1000000, domain=None, algorithm=None, *, maximum_streamline_length: float = 300.0,
+        runtime=None):
+    """Track orientation distribution from a field (__init__.py:217-366).
+
+    ``field`` is a 4D image (the local model inferred from its coefficient
+    count) or a prepared field; seeds come from the boundary of ``domain``
+    (default: the nonzero voxels of an image field) and the TOD is
+    accumulated on the field's image grid (or an image domain's grid for a
+    custom field).  Returns 45 normalised SH coefficients per voxel."""
+    if not isinstance(n_seeds, (int, __import__("numpy").integer)) or n_seeds < 0:
+        raise ValueError("n_seeds must be a non-negative integer.")
+    import numpy as np
+
+    if not np.isfinite(maximum_streamline_length) or maximum_streamline_length < 0:
+        raise ValueError("maximum_streamline_length must be finite and non-negative.")
+    grid_shape = grid_affine = grid_header = None
+    domain_image = None
+    local_model = None
+    if nifti.is_image(field):
+        if field.ndim != 4:
+            raise ValueError("The tracking image must be four-dimensional.")
+        tracking_field = field_module.Image(field)
+        domain_image = Nifti1Image(np.any(np.asanyarray(field.dataobj) != 0, axis=-1).astype(np.uint8), field.affine)
+        local_model = local.from_shape(field.shape)
+        grid_shape, grid_affine = field.shape[:3], field.affine
+        grid_header = getattr(field, "header", None)
+    elif isinstance(field, field_module.BaseField):
+        tracking_field = field
+        local_model = local.from_shape((field.n_parameters,)) if algorithm is None else None
+        if isinstance(field, field_module.Image):
+            grid_affine = np.linalg.inv(field.inverse_affine)
+            domain_image = Nifti1Image(np.any(field.values != 0, axis=-1).astype(np.uint8), grid_affine)
+            grid_shape = tuple(int(size) for size in field.values.shape[:3])
+    else:
+        raise TypeError("field must be a Nifti1Image or a BaseField instance.")
+    if algorithm is None:
+        tracking_algorithm = algorithm_module.Transport(local_model)
+    else:
+        jobs._validate_algorithm(algorithm)
+        tracking_algorithm = algorithm
+    if tracking_algorithm.local_model.n_parameters != tracking_field.n_parameters:
+        raise ValueError(
+            "Algorithm local model parameter count does not match the field: "
+            f"{tracking_algorithm.local_model.n_parameters} != {tracking_field.n_parameters}"
+        )
+    if domain is not None and not (nifti.is_image(domain) or isinstance(domain, domain_module.BaseDomain)):
+        raise TypeError("domain must be a BaseDomain, Nifti1Image, or None.")
+    tracking_domain = None
+    if nifti.is_image(domain):
+        if domain.ndim != 3:
+            raise ValueError("Domain image must be three-dimensional.")
+        domain_image = domain
+        if grid_shape is None:
+            grid_shape, grid_affine = domain.shape, domain.affine
+    elif domain is not None:
+        tracking_domain = domain
+        if grid_shape is None and isinstance(domain, domain_module.Image):
+            grid_shape = tuple(int(size) for size in domain.values.shape)
+            grid_affine = np.linalg.inv(domain.inverse_affine)
+    elif domain_image is None:
+        raise ValueError("A domain is required when the field is not an image field.")
+    if grid_shape is None or grid_affine is None:
+        raise ValueError("A field image or image-based domain is required to define the TOD grid.")
+    image_grid = Nifti1Image(np.zeros(grid_shape, dtype=np.float32), grid_affine, grid_header)
+    if tracking_domain is None:
+        if not np.any(np.asanyarray(domain_image.dataobj) != 0):
+            return Nifti1Image(np.zeros(tuple(grid_shape) + (45,), dtype=np.float32), grid_affine, grid_header)
+        tracking_domain = domain_module.Image(domain_image)
+    return tracking.tod(tracking_algorithm, tracking_domain, tracking_field, image_grid, n_seeds,
+                        maximum_streamline_length=maximum_streamline_length, runtime=runtime)
 
 
 def tractogram(

@@ -61,6 +61,7 @@ EXPORTS = (
     "tg_domain_contains",
     "tg_field_evaluate",
     "tg_boundary_seeds",
+    "tg_tod",
     "tg_local_evaluate",
     "tg_update_orientation",
     "tg_rng_stream",
@@ -163,6 +164,7 @@ def load() -> ctypes.CDLL:
         "tg_domain_contains": ([P, P, U32, P, P], ctypes.c_int),
         "tg_field_evaluate": ([P, P, U32, P, P], ctypes.c_int),
         "tg_boundary_seeds": ([P, U32, P, P, U32, U32, U32, P, P], ctypes.c_int),
+        "tg_tod": ([AP, P, P, P, U32, P, P, U32, U32, U32, P, P, P, P], ctypes.c_int),
         "tg_local_evaluate": ([I32, U32, P, P, U32, P, P], ctypes.c_int),
         "tg_update_orientation": ([I32, U32, AP, P, P, U32, P, P], ctypes.c_int),
         "tg_rng_stream": ([I32, U32, U32, U32, U32, P, P], ctypes.c_int),

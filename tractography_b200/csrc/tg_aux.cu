@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "tg_internal.h"
+#include "tg_step.cuh"
 
 namespace tg {
 
@@ -336,27 +337,9 @@ __global__ void __launch_bounds__(128) boundary_seeds_kernel(const float4* __res
     const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= n) return;
     Mwc st = rng_init(rng_seed, gid);
-    const float target = randu(st);
-    uint32_t lo = 0, hi = n_triangles;
-    while (lo < hi) {
-        const uint32_t mid = lo + (hi - lo) / 2;
-        if (cumulative[mid] <= target) lo = mid + 1;
-        else hi = mid;
-    }
-    const uint4 ix = triangles[lo < n_triangles - 1 ? lo : n_triangles - 1];
-    const float4 a = vertices[ix.x], b = vertices[ix.y], c = vertices[ix.z];
-    const float root_u = sqrtf(randu(st));
-    const float v = randu(st);
-    const float wa = 1.0f - root_u, wb = root_u * (1.0f - v), wc = root_u * v;
-    const float sx = (wa * a.x + wb * b.x) + wc * c.x;
-    const float sy = (wa * a.y + wb * b.y) + wc * c.y;
-    const float sz = (wa * a.z + wb * b.z) + wc * c.z;
-    const float e1x = b.x - a.x, e1y = b.y - a.y, e1z = b.z - a.z;
-    const float e2x = c.x - a.x, e2y = c.y - a.y, e2z = c.z - a.z;
-    const float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
-    const float len = sqrtf(nx * nx + ny * ny + nz * nz);
-    const float ox = -(nx / len), oy = -(ny / len), oz = -(nz / len);
-    out[2 * (size_t)gid] = make_float4(sx + 1e-4f * ox, sy + 1e-4f * oy, sz + 1e-4f * oz, 1.0f);
+    float px, py, pz, ox, oy, oz;
+    sample_boundary(vertices, triangles, cumulative, n_triangles, st, px, py, pz, ox, oy, oz);
+    out[2 * (size_t)gid] = make_float4(px, py, pz, 1.0f);
     out[2 * (size_t)gid + 1] = make_float4(ox, oy, oz, 0.0f);
 }
 

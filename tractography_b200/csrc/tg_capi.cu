@@ -1089,6 +1089,41 @@ int tg_boundary_seeds(const float* vertices, uint32_t n_vertices, const uint32_t
     return TG_OK;
 }
 
+int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field, const float* vertices,
+           uint32_t n_vertices, const uint32_t* triangles, const float* cumulative_areas, uint32_t n_triangles,
+           uint32_t n_seeds, uint32_t n_steps, const uint32_t out_dims[3], const float out_inverse_affine[16],
+           float* coefficients, void* stream)
+{
+    TodParams q;
+    std::memset(&q, 0, sizeof q);
+    int st = make_track_params(algorithm, domain, field, 1.0f, 1u, &q.t);
+    if (st != TG_OK) return st;
+    if (n_seeds == 0 || n_steps == 0) return TG_OK;
+    if (vertices == nullptr || triangles == nullptr || cumulative_areas == nullptr || coefficients == nullptr ||
+        out_dims == nullptr || out_inverse_affine == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    if (n_triangles == 0 || n_vertices == 0)
+        return fail(TG_ERR_INVALID_ARGUMENT, "The boundary mesh must contain at least one triangle.");
+    q.vertices = reinterpret_cast<const float4*>(vertices);
+    q.triangles = reinterpret_cast<const uint4*>(triangles);
+    q.cumulative = cumulative_areas;
+    q.n_triangles = n_triangles;
+    q.rng_seed = algorithm->rng_seed;
+    q.seed_offset = algorithm->seed_offset;
+    q.n_seeds = n_seeds;
+    q.n_steps = n_steps;
+    const Grid g = grid_of(out_inverse_affine, out_dims[0], out_dims[1], out_dims[2]);
+    q.out_row0 = g.row0;
+    q.out_row1 = g.row1;
+    q.out_row2 = g.row2;
+    q.nx = out_dims[0];
+    q.ny = out_dims[1];
+    q.nz = out_dims[2];
+    q.coefficients = coefficients;
+    TG_TRY(launch_tod(field->d.model, field->d.lmax, q, as_stream(stream)));
+    return TG_OK;
+}
+
 int tg_field_evaluate(const tg_field* field, const float* points, uint32_t n, float* out, void* stream)
 {
     if (field == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "field is null");

@@ -158,6 +158,23 @@ cudaError_t launch_track_class(const MultiParams& mp, const ClassDev& cls, int g
 int class_blocks_per_sm(int kind);
 int class_kind(int model, int lmax, int algorithm);
 
+// Track orientation distribution (tg_tod.cu, tracking.py:181-385).
+struct TodParams {
+    TrackParams t;                 // domain, field, algorithm
+    const float4* vertices;        // boundary sampler arrays (device)
+    const uint4* triangles;
+    const float* cumulative;
+    uint32_t n_triangles;
+    uint32_t rng_seed;
+    uint64_t seed_offset;          // Philox index base
+    uint32_t n_seeds;
+    uint32_t n_steps;              // floor(maximum_streamline_length / step_size)
+    float4 out_row0, out_row1, out_row2;   // output grid inverse affine rows
+    uint32_t nx, ny, nz;
+    float* coefficients;           // (nx, ny, nz, 45) float32, accumulated
+};
+cudaError_t launch_tod(int model, int lmax, const TodParams& q, cudaStream_t stream);
+
 // Boundary seeding (tg_aux.cu).
 cudaError_t launch_boundary_seeds(const float4* vertices, const uint4* triangles, const float* cumulative,
                                   uint32_t n_triangles, uint32_t rng_seed, uint32_t n, float4* out,

@@ -40,16 +40,18 @@ struct Lane {
 // closed surface, where the seed must be inside and every later point must
 // be reached by a segment from the previous one that does not hit the
 // surface (the found flag of bvh.cl:83-131).
-template <int MODEL, int LMAX, int ALGO, int CPAD, int DOM = kDomainImage>
-__device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (&c)[CPAD],
-                                          float& qx, float& qy, float& qz)
+// The domain test and the field gather of one iteration (tracking.py:123-
+// 133): false when the streamline stops; otherwise c holds the coefficients
+// of the nearest field voxel.
+template <int MODEL, int LMAX, int CPAD, int DOM>
+__device__ __forceinline__ bool locate(const TrackParams& p, Lane& s, float (&c)[CPAD])
 {
     float ax, ay, az;
     if constexpr (DOM == kDomainMesh) {
         if (s.steps == 0u) {
-            if (!mesh_contains(p.mesh, s.px, s.py, s.pz)) return 0;
+            if (!mesh_contains(p.mesh, s.px, s.py, s.pz)) return false;
         } else if (mesh_segment_blocked(p.mesh, s.lx, s.ly, s.lz, s.px, s.py, s.pz)) {
-            return 0;
+            return false;
         }
         s.lx = s.px;
         s.ly = s.py;
@@ -67,9 +69,9 @@ __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (
         if (vx != s.dvx || vy != s.dvy || vz != s.dvz) {
             if (!(vx >= 0.0f && vx < (float)p.dgrid.nx && vy >= 0.0f && vy < (float)p.dgrid.ny &&
                   vz >= 0.0f && vz < (float)p.dgrid.nz))
-                return 0;
+                return false;
             const int64_t k = ((int64_t)(int32_t)vx * p.dgrid.ny + (int32_t)vy) * p.dgrid.nz + (int32_t)vz;
-            if (__ldg(p.mask + k) == 0) return 0;
+            if (__ldg(p.mask + k) == 0) return false;
             s.dvx = vx;
             s.dvy = vy;
             s.dvz = vz;
@@ -85,7 +87,7 @@ __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (
     if (fx != s.fvx || fy != s.fvy || fz != s.fvz) {
         if (!(fx >= 0.0f && fx < (float)p.fgrid.nx && fy >= 0.0f && fy < (float)p.fgrid.ny &&
               fz >= 0.0f && fz < (float)p.fgrid.nz))
-            return 0;
+            return false;
         const int64_t fv = ((int64_t)(int32_t)fx * p.fgrid.ny + (int32_t)fy) * p.fgrid.nz + (int32_t)fz;
         const float4* src = reinterpret_cast<const float4*>(p.field) + fv * (CPAD / 4);
 #pragma unroll
@@ -100,7 +102,14 @@ __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (
         s.fvy = fy;
         s.fvz = fz;
     }
+    return true;
+}
 
+template <int MODEL, int LMAX, int ALGO, int CPAD, int DOM = kDomainImage>
+__device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (&c)[CPAD],
+                                          float& qx, float& qy, float& qz)
+{
+    if (!locate<MODEL, LMAX, CPAD, DOM>(p, s, c)) return 0;
     update_orientation<MODEL, LMAX, ALGO>(p.algo, c, s.ox, s.oy, s.oz, s.rng);
     s.steps += 1u;
 
@@ -117,6 +126,43 @@ __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (
         return 2;
     }
     return 1;
+}
+
+// domain.py:95-120 domain_sample_boundary: a point uniform over the
+// boundary's area (triangle by the normalised cumulative areas), its inward
+// normal, the point moved 1e-4 inward; three draws from st.  Vector
+// operations in the reference's order (normalize = v / length(v)).
+__device__ __forceinline__ void sample_boundary(const float4* __restrict__ vertices,
+                                               const uint4* __restrict__ triangles,
+                                               const float* __restrict__ cumulative, uint32_t n_triangles,
+                                               Mwc& st, float& px, float& py, float& pz, float& ox, float& oy,
+                                               float& oz)
+{
+    const float target = randu(st);
+    uint32_t lo = 0, hi = n_triangles;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (cumulative[mid] <= target) lo = mid + 1;
+        else hi = mid;
+    }
+    const uint4 ix = triangles[lo < n_triangles - 1 ? lo : n_triangles - 1];
+    const float4 a = vertices[ix.x], b = vertices[ix.y], c = vertices[ix.z];
+    const float root_u = sqrtf(randu(st));
+    const float v = randu(st);
+    const float wa = 1.0f - root_u, wb = root_u * (1.0f - v), wc = root_u * v;
+    const float sx = (wa * a.x + wb * b.x) + wc * c.x;
+    const float sy = (wa * a.y + wb * b.y) + wc * c.y;
+    const float sz = (wa * a.z + wb * b.z) + wc * c.z;
+    const float e1x = b.x - a.x, e1y = b.y - a.y, e1z = b.z - a.z;
+    const float e2x = c.x - a.x, e2y = c.y - a.y, e2z = c.z - a.z;
+    const float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+    const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+    ox = -(nx / len);
+    oy = -(ny / len);
+    oz = -(nz / len);
+    px = sx + 1e-4f * ox;
+    py = sy + 1e-4f * oy;
+    pz = sz + 1e-4f * oz;
 }
 
 // A live streamline handed from one round of a persistent launch to the

@@ -161,3 +161,57 @@ def tractogram_dense(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseFi
             out.ctypes.data_as(ctypes.c_void_p), lengths.ctypes.data_as(ctypes.c_void_p),
             ctypes.c_void_p(runtime.stream_handle)))
     return out, lengths
+
+
+def tod(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, image, n_seeds: int,
+        maximum_streamline_length: float = 300.0, runtime=None):
+    """Track orientation distribution as lmax-8 SH coefficients (tracking.py:181-385).
+
+    ``n_seeds`` seeds are drawn on the domain boundary (``domain.seed``'s
+    sampler, stream rng_init(rng_seed, i) with rng_seed = the algorithm's next
+    seed); each track is integrated for at most
+    floor(maximum_streamline_length / step_size) iterations and the real SH
+    basis of its orientation at every iteration is added to the output voxel
+    nearest the point on ``image``'s grid.  Each nonempty voxel is normalised
+    to unit integral.  Returns an image of shape image.shape + (45,).
+    """
+    from .nifti import Nifti1Image
+    from .utils import normalize_odf
+
+    _check_compatible(algorithm, field)
+    if not isinstance(n_seeds, (int, np.integer)) or n_seeds < 0:
+        raise ValueError("n_seeds must be a non-negative integer.")
+    if not np.isfinite(maximum_streamline_length) or maximum_streamline_length < 0:
+        raise ValueError("maximum_streamline_length must be finite and non-negative.")
+    if len(image.shape) != 3:
+        raise ValueError("The output image description must be 3D.")
+    output_shape = tuple(int(size) for size in image.shape)
+    affine = np.asarray(image.affine if image.affine is not None else np.eye(4), dtype=np.float64)
+    inverse_affine = np.ascontiguousarray(np.linalg.inv(affine), dtype=np.float32)
+    step_size = float(algorithm.step_size)
+    if not np.isfinite(step_size) or step_size <= 0:
+        raise ValueError("algorithm.step_size must be finite and positive.")
+    n_steps = int(np.floor(maximum_streamline_length / step_size))
+    raw = np.zeros(output_shape + (45,), dtype=np.float32)
+    if n_seeds > 0 and n_steps > 0:
+        from .runtime import default_runtime
+
+        runtime = runtime or default_runtime()
+        import torch
+
+        v4, f4, cumulative = domain.boundary_arrays()
+        with runtime.device_scope():
+            d_handle, f_handle = _handles(algorithm, domain, field, runtime)
+            a = to_struct(algorithm, algorithm.get_rng_seed(),
+                          algorithm.philox_key() if algorithm.rng_mode() == _lib.RNG_PHILOX else 0, 0)
+            dv, df, dc = runtime.to_device(v4), runtime.to_device(f4), runtime.to_device(cumulative)
+            coefficients = torch.zeros(output_shape + (45,), dtype=torch.float32, device=runtime.device)
+            dims = np.asarray(output_shape, dtype=np.uint32)
+            _lib.check(runtime.lib.tg_tod(
+                ctypes.byref(a), d_handle, f_handle, ctypes.c_void_p(dv.data_ptr()), len(v4),
+                ctypes.c_void_p(df.data_ptr()), ctypes.c_void_p(dc.data_ptr()), len(f4), int(n_seeds), n_steps,
+                dims.ctypes.data_as(ctypes.c_void_p), inverse_affine.ctypes.data_as(ctypes.c_void_p),
+                ctypes.c_void_p(coefficients.data_ptr()), ctypes.c_void_p(runtime.stream_handle)))
+            raw = coefficients.cpu().numpy()
+    header = getattr(image, "header", None)
+    return Nifti1Image(normalize_odf(raw).astype(np.float32), affine, header)
