@@ -308,6 +308,18 @@ int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_fiel
            uint32_t n_vertices, const uint32_t* triangles, const float* cumulative_areas, uint32_t n_triangles,
            uint32_t n_seeds, uint32_t n_steps, const uint32_t out_dims[3], const float out_inverse_affine[16],
            float* coefficients, void* stream);
+/* tracking.connectome (tracking.py:388-602): n_seeds boundary seeds
+ * (sampler arrays as for tg_boundary_seeds) tracked for at most n_steps
+ * iterations; a track that moved at least minimum_length and whose final
+ * segment hits the boundary (closest hit in `boundary`, a mesh domain made
+ * from the same vertices and faces) writes the 9 products of its start and
+ * end barycentric weights at (start vertex, end vertex) pairs into rows,
+ * columns and weights (device, 9 per seed; rows = -1 where nothing was
+ * written).  Deterministic. */
+int tg_connectome(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
+                  const tg_domain* boundary, const float* vertices, uint32_t n_vertices, const uint32_t* triangles,
+                  const float* cumulative_areas, uint32_t n_triangles, uint32_t n_seeds, uint32_t n_steps,
+                  float minimum_length, int32_t* rows, int32_t* columns, float* weights, void* stream);
 /* domain.seed, domain.py:494-575 with domain_sample_boundary (:95-120):
  * n_seeds seeds uniform over a boundary surface's area, pointing inward,
  * seed i drawing from rng_init(rng_seed, i).  Device arrays: vertices

@@ -87,6 +87,7 @@ def lib():
         _lib.tgo_segment_hits.argtypes = [P, P, P, U32, P, P, P, ctypes.c_int]
         _lib.tgo_boundary_seeds.argtypes = [P, P, P, U32, U32, U32, P]
         _lib.tgo_tod.argtypes = [P, P, P, P, U32, U32, U32, P, P, P]
+        _lib.tgo_connectome.argtypes = [P, P, P, P, P, U32, U32, U32, F, P, P, P]
         _lib.tgo_mesh_contains.argtypes = [P, F, F, F]
         _lib.tgo_mesh_contains.restype = ctypes.c_int
         _lib.tgo_bvh_count_hits.argtypes = [P, P, P]
@@ -150,6 +151,16 @@ class Case:
         lib().tgo_tod(ctypes.byref(self.p), _ptr(v), _ptr(t), _ptr(c), len(c), n_seeds, n_steps, _ptr(dims),
                       _ptr(inv), _ptr(out))
         return out
+
+    def connectome(self, boundary_bvh, boundary, n_seeds, n_steps, minimum_length=0.0):
+        """tracking.py:388-602 contributions: rows, columns, weights (9 per seed)."""
+        v, t, c = (np.ascontiguousarray(a, dt) for a, dt in zip(boundary, (np.float32, np.uint32, np.float32)))
+        rows = np.empty(9 * n_seeds, np.int32)
+        cols = np.zeros(9 * n_seeds, np.int32)
+        w = np.zeros(9 * n_seeds, np.float32)
+        lib().tgo_connectome(ctypes.byref(self.p), ctypes.byref(boundary_bvh.struct), _ptr(v), _ptr(t), _ptr(c),
+                             len(c), n_seeds, n_steps, minimum_length, _ptr(rows), _ptr(cols), _ptr(w))
+        return rows, cols, w
 
     def contains(self, points):
         pts = _points4(points)

@@ -553,8 +553,21 @@ void tgo_segment_hits(const tgo_bvh* b, const float* starts, const float* ends, 
 }
 
 /* domain.py:95-120 domain_sample_boundary, once per seed (:520-545). */
+static void sample_boundary_full(const float* vertices, const uint32_t* triangles, const float* cumulative,
+                                 uint32_t n_triangles, uint32_t st[2], float* out, uint32_t* tri_out,
+                                 float* bary_out);
+
 static void sample_boundary(const float* vertices, const uint32_t* triangles, const float* cumulative,
                             uint32_t n_triangles, uint32_t st[2], float* out)
+{
+    uint32_t tri;
+    float bary[3];
+    sample_boundary_full(vertices, triangles, cumulative, n_triangles, st, out, &tri, bary);
+}
+
+static void sample_boundary_full(const float* vertices, const uint32_t* triangles, const float* cumulative,
+                                 uint32_t n_triangles, uint32_t st[2], float* out, uint32_t* tri_out,
+                                 float* bary_out)
 {
     {
         const float target = randu(st);
@@ -570,6 +583,10 @@ static void sample_boundary(const float* vertices, const uint32_t* triangles, co
         const float* c = vertices + 4 * (size_t)triangles[4 * (size_t)tri + 2];
         const float root_u = sqrtf(randu(st));
         const float v = randu(st);
+        *tri_out = tri;
+        bary_out[0] = 1.0f - root_u;
+        bary_out[1] = root_u * (1.0f - v);
+        bary_out[2] = root_u * v;
         float p[3], e1[3], e2[3], nrm[3];
         for (int k = 0; k < 3; ++k) {
             p[k] = ((1.0f - root_u) * a[k] + (root_u * (1.0f - v)) * b[k]) + (root_u * v) * c[k];
@@ -732,6 +749,74 @@ void tgo_tod(const tgo_problem* p, const float* vertices, const uint32_t* triang
             pos[2] = fmaf(p->step_size, o[2], pos[2]);
         }
         if (prev[0] >= 0) tod_flush(coefficients, acc, prev, out_dims);
+    }
+}
+
+void tgo_connectome(const tgo_problem* p, const tgo_bvh* boundary, const float* vertices, const uint32_t* triangles,
+                    const float* cumulative, uint32_t n_triangles, uint32_t n_seeds, uint32_t n_steps,
+                    float minimum_length, int32_t* rows, int32_t* columns, float* weights)
+{
+    const uint32_t C = p->field_dims[3];
+    long g;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (g = 0; g < (long)n_seeds; ++g) {
+        const uint32_t gid = (uint32_t)g;
+        const size_t base = 9 * (size_t)gid;
+        for (int k = 0; k < 9; ++k) rows[base + k] = -1;
+        rng_t rng;
+        float seed[8], start_w[3];
+        uint32_t start_tri;
+        tgo_rng_init(p->rng_seed, gid, rng.mwc);
+        sample_boundary_full(vertices, triangles, cumulative, n_triangles, rng.mwc, seed, &start_tri, start_w);
+        rng.index = p->seed_offset + gid;
+        rng.step = 0u;
+        float pos[3] = {seed[0], seed[1], seed[2]};
+        float o[3] = {seed[4], seed[5], seed[6]};
+        float prev[3] = {pos[0], pos[1], pos[2]};
+        float last[3] = {pos[0], pos[1], pos[2]};
+        int first = 1;
+        uint32_t tracked = 0;
+        for (uint32_t step = 0; step < n_steps; ++step) {
+            if (p->mesh) {
+                if (first) {
+                    if (!tgo_mesh_contains(p->mesh, pos[0], pos[1], pos[2])) break;
+                } else {
+                    uint32_t tri;
+                    float bc[3], t;
+                    if (tgo_bvh_segment_hit(p->mesh, last, pos, &tri, bc, &t)) break;
+                }
+                first = 0;
+                last[0] = pos[0];
+                last[1] = pos[1];
+                last[2] = pos[2];
+            } else if (!domain_contains(p, pos[0], pos[1], pos[2])) {
+                break;
+            }
+            const float* c = field_voxel(p, pos[0], pos[1], pos[2]);
+            if (!c) break;
+            update_orientation(p, c, C, o, &rng);
+            const float len = sqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+            if (!(isfinite(o[0]) && isfinite(o[1]) && isfinite(o[2])) || len < 0.5f) break;
+            prev[0] = pos[0];
+            prev[1] = pos[1];
+            prev[2] = pos[2];
+            pos[0] = fmaf(p->step_size, o[0], pos[0]);
+            pos[1] = fmaf(p->step_size, o[1], pos[1]);
+            pos[2] = fmaf(p->step_size, o[2], pos[2]);
+            tracked++;
+        }
+        if ((float)tracked * p->step_size < minimum_length) continue;
+        uint32_t hit_tri;
+        float end_w[3], t;
+        if (!tgo_bvh_segment_hit(boundary, prev, pos, &hit_tri, end_w, &t)) continue;
+        const uint32_t* sv = triangles + 4 * (size_t)start_tri;
+        const uint32_t* ev = triangles + 4 * (size_t)hit_tri;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                rows[base + 3 * i + j] = (int32_t)sv[i];
+                columns[base + 3 * i + j] = (int32_t)ev[j];
+                weights[base + 3 * i + j] = start_w[i] * end_w[j];
+            }
     }
 }
 

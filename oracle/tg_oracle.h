@@ -126,6 +126,13 @@ void tgo_tod(const tgo_problem* p, const float* vertices, const uint32_t* triang
              uint32_t n_triangles, uint32_t n_seeds, uint32_t n_steps, const uint32_t out_dims[3],
              const float out_inverse_affine[16], float* coefficients);
 
+/* tracking.py:388-602 (connectome): per seed, 9 (row, column, weight)
+ * contributions (rows -1 when none) from the start barycentric weights and
+ * the closest boundary hit of the final segment in `boundary`. */
+void tgo_connectome(const tgo_problem* p, const tgo_bvh* boundary, const float* vertices, const uint32_t* triangles,
+                    const float* cumulative, uint32_t n_triangles, uint32_t n_seeds, uint32_t n_steps,
+                    float minimum_length, int32_t* rows, int32_t* columns, float* weights);
+
 /* core.cl:180-245 primitives. */
 void tgo_rng_init(uint32_t seed, uint32_t stream_id, uint32_t state[2]);
 void tgo_randu_stream(uint32_t s0, uint32_t s1, uint32_t n, float* out);

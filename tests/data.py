@@ -69,6 +69,17 @@ def cross(shape=(10, 10, 1), n_coefficients=45):
     return fod, tg.Nifti1Image(mask, np.eye(4))
 
 
+def cross_segmentation(shape=(10, 10, 1)):
+    """Regions 1-4 at the four ends of the cross (test/data/__init__.py:86-92)."""
+    xo, yo = shape[0] // 3, shape[1] // 3
+    seg = np.zeros(shape, dtype=np.uint8)
+    seg[xo:-xo, 0] = 1
+    seg[xo:-xo, -1] = 2
+    seg[0, yo:-yo] = 3
+    seg[-1, yo:-yo] = 4
+    return tg.Nifti1Image(seg, np.eye(4))
+
+
 def tensor_circle(shape=(20, 20, 1), radius=5, width=2):
     values = np.zeros(shape + (6,))
     values[..., :3] = 0.003

@@ -29,8 +29,110 @@ seeds_module = seeds
 __all__ = [
     "ArraySequence", "BufferAccess", "CudaRuntime", "Nifti1Image", "OpenCLRuntime", "Tractogram",
     "algorithm", "core", "domain", "field", "jobs", "load_tck", "local", "nifti", "save_tck", "seeds",
-    "streamlines", "tod", "tracking", "tractogram", "utils",
+    "connectome", "streamlines", "tod", "tracking", "tractogram", "utils",
 ]
+
+
+def connectome(field, n_seeds: int = 1000000, domain=None, algorithm=None, segmentation=None, *,
+               distance_upper_bound: float = 4.0, maximum_streamline_length: float = 300.0,
+               minimum_streamline_length: float = 0.0, runtime=None):
+    """Boundary or region connectome (__init__.py:45-214).
+
+    Without ``segmentation``: the directed boundary-vertex connectome (CSR)
+    and the vertex indices.  With a segmentation of positive labels: boundary
+    vertices are assigned to their nearest labelled voxel within
+    ``distance_upper_bound`` and the matrix is aggregated by region (dense,
+    not symmetrised), with the labels."""
+    import numpy as np
+    from scipy.sparse import csr_matrix
+    from scipy.spatial import cKDTree
+
+    from .nifti import apply_affine
+
+    if not isinstance(n_seeds, (int, np.integer)) or n_seeds < 0:
+        raise ValueError("n_seeds must be a non-negative integer.")
+    if not np.isfinite(distance_upper_bound) or distance_upper_bound < 0:
+        raise ValueError("distance_upper_bound must be finite and non-negative.")
+    if not np.isfinite(maximum_streamline_length) or maximum_streamline_length < 0:
+        raise ValueError("maximum_streamline_length must be finite and non-negative.")
+    if not np.isfinite(minimum_streamline_length) or minimum_streamline_length < 0:
+        raise ValueError("minimum_streamline_length must be finite and non-negative.")
+    if minimum_streamline_length > maximum_streamline_length:
+        raise ValueError("minimum_streamline_length must not exceed maximum_streamline_length.")
+    seg_data = labels = None
+    if segmentation is not None:
+        if not nifti.is_image(segmentation):
+            raise TypeError("segmentation must be a Nifti1Image or None.")
+        seg_data = np.asanyarray(segmentation.dataobj)
+        if seg_data.ndim != 3:
+            raise ValueError("Segmentation image must be three-dimensional.")
+        labels = np.unique(seg_data[seg_data > 0])
+        labels = labels[labels > 0]
+        if len(labels) == 0:
+            return np.zeros((0, 0), dtype=np.float32), labels
+    domain_image = None
+    local_model = None
+    if nifti.is_image(field):
+        if field.ndim != 4:
+            raise ValueError("The tracking image must be four-dimensional.")
+        tracking_field = field_module.Image(field)
+        domain_image = Nifti1Image(np.any(np.asanyarray(field.dataobj) != 0, axis=-1).astype(np.uint8), field.affine)
+        local_model = local.from_shape(field.shape)
+    elif isinstance(field, field_module.BaseField):
+        tracking_field = field
+        local_model = local.from_shape((field.n_parameters,)) if algorithm is None else None
+        if isinstance(field, field_module.Image):
+            domain_image = Nifti1Image(np.any(field.values != 0, axis=-1).astype(np.uint8),
+                                       np.linalg.inv(field.inverse_affine))
+    else:
+        raise TypeError("field must be a Nifti1Image or a BaseField instance.")
+    if algorithm is None:
+        tracking_algorithm = algorithm_module.Transport(local_model)
+    else:
+        jobs._validate_algorithm(algorithm)
+        tracking_algorithm = algorithm
+    if tracking_algorithm.local_model.n_parameters != tracking_field.n_parameters:
+        raise ValueError(
+            "Algorithm local model parameter count does not match the field: "
+            f"{tracking_algorithm.local_model.n_parameters} != {tracking_field.n_parameters}"
+        )
+    if domain is not None and not (nifti.is_image(domain) or isinstance(domain, domain_module.BaseDomain)):
+        raise TypeError("domain must be a BaseDomain, Nifti1Image, or None.")
+    if nifti.is_image(domain):
+        tracking_domain = domain_module.Image(domain)
+    elif domain is not None:
+        tracking_domain = domain
+    elif domain_image is not None:
+        if not np.any(np.asanyarray(domain_image.dataobj) != 0):
+            if labels is None:
+                return csr_matrix((0, 0), dtype=np.float32), np.empty(0, dtype=np.intp)
+            return np.zeros((len(labels), len(labels)), dtype=np.float32), labels
+        tracking_domain = domain_module.Image(domain_image)
+    else:
+        raise ValueError("A domain is required when the field is not an image field.")
+    boundary_matrix = tracking.connectome(tracking_algorithm, tracking_domain, tracking_field, n_seeds,
+                                          maximum_streamline_length=maximum_streamline_length,
+                                          minimum_streamline_length=minimum_streamline_length, runtime=runtime)
+    if labels is None:
+        return boundary_matrix, np.arange(boundary_matrix.shape[0], dtype=np.intp)
+    voxel_indices = np.argwhere(seg_data > 0)
+    affine = segmentation.affine if segmentation.affine is not None else np.eye(4)
+    vertices = tracking_domain.boundary.vertices
+    distances, nearest = cKDTree(apply_affine(affine, voxel_indices)).query(
+        vertices, distance_upper_bound=distance_upper_bound)
+    distances = np.asarray(distances).reshape(-1)
+    nearest = np.asarray(nearest, dtype=np.intp).reshape(-1)
+    assigned = np.isfinite(distances)
+    label_index = {label: k for k, label in enumerate(labels)}
+    vertex_labels = np.zeros(len(vertices), dtype=np.intp)
+    hit = voxel_indices[nearest[assigned]]
+    vertex_labels[assigned] = np.fromiter((label_index[x] for x in seg_data[hit[:, 0], hit[:, 1], hit[:, 2]]),
+                                          dtype=np.intp, count=int(np.count_nonzero(assigned)))
+    selected = np.flatnonzero(assigned)
+    assignment = csr_matrix((np.ones(len(selected), dtype=np.float32), (vertex_labels[selected], selected)),
+                            shape=(len(labels), len(vertex_labels)))
+    matrix = (assignment @ boundary_matrix @ assignment.T).tocsr()
+    return matrix.toarray(), labels
 
 
 def tod(field, n_seeds: int = 1000000, domain=None, algorithm=None, *, maximum_streamline_length: float = 300.0,

@@ -1124,6 +1124,42 @@ int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_fiel
     return TG_OK;
 }
 
+int tg_connectome(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
+                  const tg_domain* boundary, const float* vertices, uint32_t n_vertices, const uint32_t* triangles,
+                  const float* cumulative_areas, uint32_t n_triangles, uint32_t n_seeds, uint32_t n_steps,
+                  float minimum_length, int32_t* rows, int32_t* columns, float* weights, void* stream)
+{
+    ConnectomeParams q;
+    std::memset(&q, 0, sizeof q);
+    int st = make_track_params(algorithm, domain, field, 1.0f, 1u, &q.t);
+    if (st != TG_OK) return st;
+    if (n_seeds == 0) return TG_OK;
+    if (boundary == nullptr || boundary->d.kind != kDomainMesh)
+        return fail(TG_ERR_INVALID_ARGUMENT, "boundary must be a mesh domain of the boundary surface");
+    if (vertices == nullptr || triangles == nullptr || cumulative_areas == nullptr || rows == nullptr ||
+        columns == nullptr || weights == nullptr)
+        return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    if (n_triangles == 0 || n_vertices == 0)
+        return fail(TG_ERR_INVALID_ARGUMENT, "The boundary mesh must contain at least one triangle.");
+    if (boundary->d.n_triangles != n_triangles)
+        return fail(TG_ERR_INVALID_ARGUMENT, "boundary BVH and sampler arrays describe different triangles");
+    q.vertices = reinterpret_cast<const float4*>(vertices);
+    q.triangles = reinterpret_cast<const uint4*>(triangles);
+    q.cumulative = cumulative_areas;
+    q.n_triangles = n_triangles;
+    q.bvh = boundary->d.mesh;
+    q.rng_seed = algorithm->rng_seed;
+    q.seed_offset = algorithm->seed_offset;
+    q.n_seeds = n_seeds;
+    q.n_steps = n_steps;
+    q.minimum_length = minimum_length;
+    q.rows = rows;
+    q.columns = columns;
+    q.weights = weights;
+    TG_TRY(launch_connectome(field->d.model, field->d.lmax, q, as_stream(stream)));
+    return TG_OK;
+}
+
 int tg_field_evaluate(const tg_field* field, const float* points, uint32_t n, float* out, void* stream)
 {
     if (field == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "field is null");

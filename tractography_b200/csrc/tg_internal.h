@@ -175,6 +175,25 @@ struct TodParams {
 };
 cudaError_t launch_tod(int model, int lmax, const TodParams& q, cudaStream_t stream);
 
+// Boundary connectome (tg_connectome.cu, tracking.py:388-602).
+struct ConnectomeParams {
+    TrackParams t;                 // domain, field, algorithm
+    const float4* vertices;        // boundary sampler arrays (device)
+    const uint4* triangles;
+    const float* cumulative;
+    uint32_t n_triangles;
+    MeshDev bvh;                   // BVH of the same boundary triangles
+    uint32_t rng_seed;
+    uint64_t seed_offset;
+    uint32_t n_seeds;
+    uint32_t n_steps;
+    float minimum_length;
+    int32_t* rows;                 // 9 per seed, -1 when the track contributes nothing
+    int32_t* columns;
+    float* weights;
+};
+cudaError_t launch_connectome(int model, int lmax, const ConnectomeParams& q, cudaStream_t stream);
+
 // Boundary seeding (tg_aux.cu).
 cudaError_t launch_boundary_seeds(const float4* vertices, const uint4* triangles, const float* cumulative,
                                   uint32_t n_triangles, uint32_t rng_seed, uint32_t n, float4* out,

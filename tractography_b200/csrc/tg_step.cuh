@@ -136,7 +136,7 @@ __device__ __forceinline__ void sample_boundary(const float4* __restrict__ verti
                                                const uint4* __restrict__ triangles,
                                                const float* __restrict__ cumulative, uint32_t n_triangles,
                                                Mwc& st, float& px, float& py, float& pz, float& ox, float& oy,
-                                               float& oz)
+                                               float& oz, uint32_t* triangle = nullptr, float* bary = nullptr)
 {
     const float target = randu(st);
     uint32_t lo = 0, hi = n_triangles;
@@ -145,11 +145,18 @@ __device__ __forceinline__ void sample_boundary(const float4* __restrict__ verti
         if (cumulative[mid] <= target) lo = mid + 1;
         else hi = mid;
     }
-    const uint4 ix = triangles[lo < n_triangles - 1 ? lo : n_triangles - 1];
+    const uint32_t tri = lo < n_triangles - 1 ? lo : n_triangles - 1;
+    const uint4 ix = triangles[tri];
     const float4 a = vertices[ix.x], b = vertices[ix.y], c = vertices[ix.z];
     const float root_u = sqrtf(randu(st));
     const float v = randu(st);
     const float wa = 1.0f - root_u, wb = root_u * (1.0f - v), wc = root_u * v;
+    if (triangle != nullptr) {
+        *triangle = tri;
+        bary[0] = wa;
+        bary[1] = wb;
+        bary[2] = wc;
+    }
     const float sx = (wa * a.x + wb * b.x) + wc * c.x;
     const float sy = (wa * a.y + wb * b.y) + wc * c.y;
     const float sz = (wa * a.z + wb * b.z) + wc * c.z;

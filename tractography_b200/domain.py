@@ -39,6 +39,28 @@ class BaseDomain(ABC):
         """(vertices (V, 3) float64, faces (F, 3)) of the domain's boundary surface."""
         raise NotImplementedError(f"{type(self).__name__} has no boundary surface")
 
+    @property
+    def boundary(self):
+        """The boundary surface (``vertices``, ``faces``), as the reference's
+        ``domain.boundary`` mesh; rows and columns of the boundary connectome
+        follow its vertex order."""
+        from types import SimpleNamespace
+
+        vertices, faces = self.boundary_mesh()
+        return SimpleNamespace(vertices=vertices, faces=faces)
+
+    def boundary_bvh(self):
+        """The boundary surface as a ``Mesh`` (its BVH answers end-segment hits)."""
+        cached = getattr(self, "_boundary_bvh", None)
+        if cached is None:
+            if isinstance(self, Mesh):
+                cached = self
+            else:
+                vertices, faces = self.boundary_mesh()
+                cached = Mesh(vertices, faces)
+            self._boundary_bvh = cached
+        return cached
+
     def boundary_arrays(self):
         """The boundary sampler's arrays (domain.py:44-70): float32 vertices
         (V, 4), uint32 kept faces (T, 4) and float32 normalised cumulative

@@ -215,3 +215,71 @@ def tod(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, image, n
             raw = coefficients.cpu().numpy()
     header = getattr(image, "header", None)
     return Nifti1Image(normalize_odf(raw).astype(np.float32), affine, header)
+
+
+def connectome(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, n_seeds: int,
+               maximum_streamline_length: float = 300.0, minimum_streamline_length: float = 0.0, runtime=None):
+    """Directed piecewise-linear boundary connectome (tracking.py:388-602).
+
+    Tracks start on the domain boundary (``domain.seed``'s sampler); when a
+    track stops for any reason its final segment is tested against the
+    boundary BVH, and a track that moved at least ``minimum_streamline_length``
+    and hit the boundary adds the outer product of its start and end
+    barycentric weights at the two triangles' vertices.  Returns a float32
+    (n_vertices, n_vertices) CSR matrix over ``domain.boundary.vertices``.
+    """
+    from scipy.sparse import coo_matrix, csr_matrix
+
+    _check_compatible(algorithm, field)
+    if not isinstance(n_seeds, (int, np.integer)) or n_seeds < 0:
+        raise ValueError("n_seeds must be a non-negative integer.")
+    if not np.isfinite(maximum_streamline_length) or maximum_streamline_length < 0:
+        raise ValueError("maximum_streamline_length must be finite and non-negative.")
+    if not np.isfinite(minimum_streamline_length) or minimum_streamline_length < 0:
+        raise ValueError("minimum_streamline_length must be finite and non-negative.")
+    if minimum_streamline_length > maximum_streamline_length:
+        raise ValueError("minimum_streamline_length must not exceed maximum_streamline_length.")
+    n_vertices = len(domain.boundary.vertices)
+    if n_seeds == 0 or n_vertices == 0:
+        return csr_matrix((n_vertices, n_vertices), dtype=np.float32)
+    step_size = float(algorithm.step_size)
+    if not np.isfinite(step_size) or step_size <= 0:
+        raise ValueError("algorithm.step_size must be finite and positive.")
+    n_steps = int(np.floor(maximum_streamline_length / step_size))
+    if n_steps == 0:
+        return csr_matrix((n_vertices, n_vertices), dtype=np.float32)
+    from .runtime import default_runtime
+
+    runtime = runtime or default_runtime()
+    import torch
+
+    v4, f4, cumulative = domain.boundary_arrays()
+    with runtime.device_scope():
+        d_handle, f_handle = _handles(algorithm, domain, field, runtime)
+        b_handle = domain.boundary_bvh().device(runtime)
+        a = to_struct(algorithm, algorithm.get_rng_seed(),
+                      algorithm.philox_key() if algorithm.rng_mode() == _lib.RNG_PHILOX else 0, 0)
+        dv, df, dc = runtime.to_device(v4), runtime.to_device(f4), runtime.to_device(cumulative)
+        rows = runtime.empty((9 * int(n_seeds),), torch.int32)
+        cols = runtime.empty((9 * int(n_seeds),), torch.int32)
+        weights = runtime.empty((9 * int(n_seeds),), torch.float32)
+        _lib.check(runtime.lib.tg_connectome(
+            ctypes.byref(a), d_handle, f_handle, b_handle, ctypes.c_void_p(dv.data_ptr()), len(v4),
+            ctypes.c_void_p(df.data_ptr()), ctypes.c_void_p(dc.data_ptr()), len(f4), int(n_seeds), n_steps,
+            float(minimum_streamline_length), ctypes.c_void_p(rows.data_ptr()), ctypes.c_void_p(cols.data_ptr()),
+            ctypes.c_void_p(weights.data_ptr()), ctypes.c_void_p(runtime.stream_handle)))
+        rows, cols, weights = rows.cpu().numpy(), cols.cpu().numpy(), weights.cpu().numpy()
+    return contributions_to_matrix(rows, cols, weights, n_vertices)
+
+
+def contributions_to_matrix(rows, cols, weights, n_vertices):
+    """Sum the kernel's (row, column, weight) contributions into a CSR matrix."""
+    from scipy.sparse import coo_matrix, csr_matrix
+
+    valid = rows >= 0
+    if not np.any(valid):
+        return csr_matrix((n_vertices, n_vertices), dtype=np.float32)
+    matrix = coo_matrix((weights[valid], (rows[valid], cols[valid])), shape=(n_vertices, n_vertices),
+                        dtype=np.float32).tocsr()
+    matrix.sum_duplicates()
+    return matrix
