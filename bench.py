@@ -789,7 +789,7 @@ def run_serve(args):
             rng = np.random.default_rng(int(rate * 1000))
             n_req = max(5, int(rate * args.duration))
             arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
-            requests = [make_request(volumes, rng) for _ in range(n_req)]
+            offered = 0
             server = Server(runtime, hbm_budget_bytes=150e9 - resident, pool_points=256 << 20, epoch_steps=1024,
                             max_requests=512)
             latency, seeds_done = [], 0
@@ -798,7 +798,9 @@ def run_serve(args):
             while len(latency) < n_req:
                 now = time.perf_counter() - t0
                 while submitted < n_req and arrivals[submitted] <= now:
-                    server.submit(requests[submitted])
+                    job = make_request(volumes, rng)
+                    offered += job.n_seeds
+                    server.submit(job)
                     submitted += 1
                 finished = server.poll()
                 for rid in finished:
@@ -816,7 +818,7 @@ def run_serve(args):
                           "steps": st.steps, "epochs": st.epochs, "busy_s": st.busy_seconds, "wall_s": wall,
                           "steps_per_s": st.steps / max(1e-9, st.busy_seconds),
                           "streamlines_per_s": seeds_done / max(1e-9, st.busy_seconds),
-                          "offered_seeds_per_s": float(sum(r.n_seeds for r in requests) / arrivals[-1])})
+                          "offered_seeds_per_s": float(offered / arrivals[-1])})
             print(json.dumps({"rate": rate, **sweep[-1]}), file=sys.stderr, flush=True)
     best = max(x["steps_per_s"] for x in sweep)
     line = {"metric": METRIC, "value": best, "unit": UNIT, "n_gpus": 1, "steps": len(rates), "warmup": 0,

@@ -219,7 +219,9 @@ int tg_tracker_get_tuning(const tg_tracker* tracker, uint32_t* blocks_per_sm, ui
 /* Continuous-batching server.  No reference counterpart (the reference
  * tracks one tg.tractogram call at a time).  Fields, domains and surfaces
  * stay resident as ordinary handles; requests (tg_job with HOST seeds and
- * batch seeds, copied at submission) are admitted in arrival order while a
+ * batch seeds, which the caller keeps valid until the request is reported
+ * finished; they are copied to the device at admission) are admitted in
+ * arrival order while a
  * request slot is free and the server's memory -- the shared point pool,
  * per-request buffers and unclaimed results -- fits in hbm_budget_bytes.
  * Each tg_server_poll runs one epoch: one persistent launch per code path

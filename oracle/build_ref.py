@@ -13,9 +13,10 @@ becomes a run-time value, and one counter increment is inserted before the
 orientation update so accepted steps can be counted.  oracle/clshim.hpp
 supplies the OpenCL built-ins.  g++ compiles each variant in its own
 translation unit and namespace; the outputs go only to oracle/_ref/.
-The boundary BVH traversal (utils/bvh.cl) and the boundary sampler of
-domain.seed are compiled the same way with batch drivers, for the BVH hit
-and boundary-seeding parity tests.
+The boundary BVH traversal (utils/bvh.cl), the boundary sampler of
+domain.seed and the `tod` and `connectome` kernels (SH lmax 8, image
+domain) are compiled the same way with batch drivers, for the BVH hit,
+boundary-seeding, TOD and connectome parity tests.
 
 Nothing from the reference is copied into this repository: the sources are
 read from the reference tree at build time.
@@ -257,6 +258,84 @@ def capture_seed(ref):
     raise RuntimeError("the reference did not build a program")
 
 
+PRODUCT_VARIANTS = [("sh45_transport", "transport"), ("sh45_diffusion", "diffusion")]
+
+TOD_DRIVER = """
+extern "C" void tgref_{name}(const float* bv, const unsigned int* bi, const float* bc, unsigned int n_tri,
+        const float* bmin, const float* bmax, const int* nodes, const unsigned int* ordered, unsigned int n_nodes,
+        const int* mask, const unsigned int* mdims, const float* minv, const float* field, const unsigned int* fdims,
+        const float* finv, float step, float gamma, float noise, unsigned int rng_seed, unsigned int n_seeds,
+        unsigned int n_steps, const unsigned int* odims, const float* oinv, float* coefficients, int threads)
+{{
+    (void)noise;
+    tgref_n_steps = n_steps;
+    long g;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : 1)
+    for (g = 0; g < (long)n_seeds; ++g) {{
+        tgref_global_id = (size_t)g;
+        {name}::tod((const float4*)bv, (const uint4*)bi, bc, n_tri, (const float4*)bmin, (const float4*)bmax,
+            (const int4*)nodes, ordered, n_nodes, mask, make_uint3(mdims[0], mdims[1], mdims[2]), (const float4*)minv,
+            field, make_uint4(fdims[0], fdims[1], fdims[2], fdims[3]), (const float4*)finv, step, gamma{noise_arg},
+            rng_seed, n_seeds, make_uint4(odims[0], odims[1], odims[2], 0u), (const float4*)oinv, coefficients);
+    }}
+}}
+"""
+
+CONNECTOME_DRIVER = """
+extern "C" void tgref_{name}(const float* bv, const unsigned int* bi, const float* bc, unsigned int n_tri,
+        const float* bmin, const float* bmax, const int* nodes, const unsigned int* ordered, unsigned int n_nodes,
+        const int* mask, const unsigned int* mdims, const float* minv, const float* field, const unsigned int* fdims,
+        const float* finv, float step, float gamma, float noise, unsigned int rng_seed, unsigned int n_seeds,
+        unsigned int n_steps, float minimum_length, int* rows, int* columns, float* weights, int threads)
+{{
+    (void)noise;
+    tgref_n_steps = n_steps;
+    long g;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : 1)
+    for (g = 0; g < (long)n_seeds; ++g) {{
+        tgref_global_id = (size_t)g;
+        {name}::connectome((const float4*)bv, (const uint4*)bi, bc, n_tri, (const float4*)bmin, (const float4*)bmax,
+            (const int4*)nodes, ordered, n_nodes, mask, make_uint3(mdims[0], mdims[1], mdims[2]),
+            (const float4*)minv, field, make_uint4(fdims[0], fdims[1], fdims[2], fdims[3]), (const float4*)finv,
+            step, gamma{noise_arg}, rng_seed, n_seeds, minimum_length, rows, columns, weights);
+    }}
+}}
+"""
+
+
+def _product_objects(ref, algorithm):
+    Image = sys.modules["nibabel.nifti1"].Nifti1Image
+    field = ref.field.Image(Image(np.ones((2, 2, 2, 45), np.float32), np.eye(4)))
+    domain = ref.domain.Image(Image(np.ones((2, 2, 2), np.uint8), np.eye(4)))
+    local = ref.local.RealSymmetricSphericalHarmonics(45)
+    alg = ref.algorithm.Transport(local, step_size=1.0) if algorithm == "transport" else \
+        ref.algorithm.Diffusion(local, step_size=1.0)
+    return field, domain, alg, Image
+
+
+def capture_tod(ref, algorithm):
+    """The reference's `tod` kernel source (tracking.py:255-356)."""
+    field, domain, alg, Image = _product_objects(ref, algorithm)
+    rt = RecordingRuntime()
+    try:
+        ref.tracking.tod(alg, domain, field, Image(np.zeros((2, 2, 2), np.float32), np.eye(4)), 1,
+                         maximum_streamline_length=float(N_STEPS_SENTINEL), runtime=rt)
+    except _Captured:
+        return rt.source
+    raise RuntimeError("the reference did not build a program")
+
+
+def capture_connectome(ref, algorithm):
+    """The reference's `connectome` kernel source (tracking.py:458-553)."""
+    field, domain, alg, _ = _product_objects(ref, algorithm)
+    rt = RecordingRuntime()
+    try:
+        ref.tracking.connectome(alg, domain, field, 1, maximum_streamline_length=float(N_STEPS_SENTINEL), runtime=rt)
+    except _Captured:
+        return rt.source
+    raise RuntimeError("the reference did not build a program")
+
+
 def bvh_source(kernel_dir):
     """utils/bvh.cl (the boundary BVH traversal) as C++ with a batch driver."""
     text = rewrite_literals(inline_includes((kernel_dir / "utils" / "bvh.cl").read_text(), kernel_dir))
@@ -297,6 +376,15 @@ def main():
     bpath = OUT / "tgref_bvh.cpp"
     bpath.write_text(bvh_source(kernel_dir))
     sources.append(bpath)
+    for name, algorithm in PRODUCT_VARIANTS:
+        noise_arg = ", noise" if algorithm == "diffusion" else ""
+        for kind, capture_fn, driver in (("tod", capture_tod, TOD_DRIVER),
+                                         ("connectome", capture_connectome, CONNECTOME_DRIVER)):
+            tname = f"{kind}_{name}"
+            path = OUT / f"tgref_{tname}.cpp"
+            path.write_text(to_cpp(capture_fn(ref, algorithm), kernel_dir, tname) +
+                            driver.format(name=tname, noise_arg=noise_arg))
+            sources.append(path)
     spath = OUT / "tgref_seed.cpp"
     spath.write_text(to_cpp(capture_seed(ref), kernel_dir, "seedref").replace(
         "extern unsigned int tgref_n_steps;", "") + SEED_DRIVER)

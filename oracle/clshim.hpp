@@ -160,6 +160,21 @@ static inline int3 convert_int3(float3 v) { return make_int3((int)v.x, (int)v.y,
 
 static inline uint mul_hi(uint a, uint b) { return (uint)(((unsigned long long)a * b) >> 32); }
 
+// Relational built-ins on vectors: -1 (all bits) for true, 0 for false;
+// all() tests the sign bit of every component.
+static inline bool isfinite(float x) { return std::isfinite(x); }
+static inline int3 isfinite(float3 v)
+{
+    return make_int3(std::isfinite(v.x) ? -1 : 0, std::isfinite(v.y) ? -1 : 0, std::isfinite(v.z) ? -1 : 0);
+}
+static inline int4 isfinite(float4 v)
+{
+    return make_int4(std::isfinite(v.x) ? -1 : 0, std::isfinite(v.y) ? -1 : 0, std::isfinite(v.z) ? -1 : 0,
+                     std::isfinite(v.w) ? -1 : 0);
+}
+static inline int all(int3 v) { return v.x < 0 && v.y < 0 && v.z < 0; }
+static inline int all(int4 v) { return v.x < 0 && v.y < 0 && v.z < 0 && v.w < 0; }
+
 static inline uint atomic_cmpxchg(volatile uint* p, uint cmp, uint val)
 {
     __atomic_compare_exchange_n(const_cast<uint*>(p), &cmp, val, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);

@@ -126,3 +126,52 @@ def boundary_seeds(vertices4, triangles4, cumulative, rng_seed, n):
     fn(v.ctypes.data, t.ctypes.data, c.ctypes.data, len(c), rng_seed & 0xFFFFFFFF, n, loc.ctypes.data,
        ori.ctypes.data)
     return np.hstack((loc, ori))
+
+
+def _domain_arrays(domain, bvh):
+    boundary = domain.boundary_arrays()
+    mask = np.ascontiguousarray(np.asarray(domain.values) != 0, dtype=np.int32)
+    arrays = [*boundary, bvh.bounds_min, bvh.bounds_max, bvh.nodes, bvh.ordered, mask,
+              np.array(mask.shape, np.uint32), np.ascontiguousarray(domain.inverse_affine, np.float32)]
+    return arrays, len(boundary[2]), len(bvh.nodes)
+
+
+def _product(kind, algorithm_kind, domain, field, bvh, step, gamma, noise, rng_seed, n_seeds, n_steps, tail, threads):
+    fld = np.ascontiguousarray(field.values, np.float32)
+    arrays, n_tri, n_nodes = _domain_arrays(domain, bvh)
+    fdims = np.array(fld.shape, np.uint32)
+    finv = np.ascontiguousarray(field.inverse_affine, np.float32)
+    fn = getattr(lib(), f"tgref_{kind}_sh45_{algorithm_kind}")
+    P, U, F = ctypes.c_void_p, ctypes.c_uint, ctypes.c_float
+    v, t, c, bmin, bmax, nodes, ordered, mask, mdims, minv = arrays
+    args = [v.ctypes.data, t.ctypes.data, c.ctypes.data, n_tri, bmin.ctypes.data, bmax.ctypes.data, nodes.ctypes.data,
+            ordered.ctypes.data, n_nodes, mask.ctypes.data, mdims.ctypes.data, minv.ctypes.data, fld.ctypes.data,
+            fdims.ctypes.data, finv.ctypes.data, step, gamma, noise, rng_seed & 0xFFFFFFFF, n_seeds, n_steps]
+    types = [P, P, P, U, P, P, P, P, U, P, P, P, P, P, P, F, F, F, U, U, U]
+    return fn, args, types, (fld, arrays, fdims, finv)
+
+
+def tod(domain, field, bvh, algorithm_kind, step, gamma, noise, rng_seed, n_seeds, n_steps, out_shape, out_inverse,
+        threads=1):
+    """The reference's `tod` kernel (SH lmax 8, image domain): raw (X, Y, Z, 45) coefficients."""
+    fn, args, types, keep = _product("tod", algorithm_kind, domain, field, bvh, step, gamma, noise, rng_seed, n_seeds,
+                                     n_steps, None, threads)
+    odims = np.array(out_shape, np.uint32)
+    oinv = np.ascontiguousarray(out_inverse, np.float32)
+    out = np.zeros(tuple(out_shape) + (45,), np.float32)
+    fn.argtypes = types + [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    fn(*args, odims.ctypes.data, oinv.ctypes.data, out.ctypes.data, threads)
+    return out
+
+
+def connectome(domain, field, bvh, algorithm_kind, step, gamma, noise, rng_seed, n_seeds, n_steps, minimum_length,
+               threads=1):
+    """The reference's `connectome` kernel (SH lmax 8, image domain): rows, columns, weights (9 per seed)."""
+    fn, args, types, keep = _product("connectome", algorithm_kind, domain, field, bvh, step, gamma, noise, rng_seed,
+                                     n_seeds, n_steps, None, threads)
+    rows = np.empty(9 * n_seeds, np.int32)
+    cols = np.zeros(9 * n_seeds, np.int32)
+    w = np.zeros(9 * n_seeds, np.float32)
+    fn.argtypes = types + [ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    fn(*args, minimum_length, rows.ctypes.data, cols.ctypes.data, w.ctypes.data, threads)
+    return rows, cols, w

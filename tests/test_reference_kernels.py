@@ -127,3 +127,60 @@ def test_boundary_seeds_match_reference_kernel(name):
         want = R.boundary_seeds(*args, rng_seed, 3000)
         got = O.boundary_seeds(*args, rng_seed, 3000)
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def _cross_case():
+    import data as _data
+
+    fod, mask = _data.cross(shape=(12, 12, 3))
+    field, domain = tg.field.Image(fod), tg.domain.Image(mask)
+    b = domain.boundary_bvh()
+    return field, domain, O.BoundaryBvh.build(b.vertices, b.faces)
+
+
+@pytest.mark.parametrize("gamma", [0.0, 1.0])
+def test_tod_transport_matches_reference_kernel(gamma):
+    """tracking.py:255-356 (the reference's own tod kernel) vs the oracle: sums agree to float tolerance."""
+    field, domain, bvh = _cross_case()
+    alg = tg.algorithm.Transport(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.1, gamma=gamma)
+    ref = R.tod(domain, field, bvh, "transport", 0.1, gamma, 0.0, 99, 3000, 80, (12, 12, 3), np.eye(4), threads=8)
+    got = oracle_case(alg, domain, field, rng_seed=99).tod(domain.boundary_arrays(), 3000, 80, (12, 12, 3),
+                                                           np.eye(4))
+    assert np.abs(ref - got).sum() <= 1e-4 * np.abs(ref).sum()
+
+
+def test_connectome_transport_matches_reference_kernel():
+    """tracking.py:458-553: same start/end vertices for >= 99.9 % of tracks, weights to float tolerance."""
+    field, domain, bvh = _cross_case()
+    alg = tg.algorithm.Transport(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.1, gamma=1.0)
+    r2, c2, w2 = R.connectome(domain, field, bvh, "transport", 0.1, 1.0, 0.0, 99, 20000, 120, 0.5, threads=8)
+    r1, c1, w1 = oracle_case(alg, domain, field, rng_seed=99).connectome(bvh, domain.boundary_arrays(), 20000, 120,
+                                                                         0.5)
+    assert np.mean(r1 == r2) >= 0.999
+    same = (r1 == r2) & (r1 >= 0)
+    assert np.mean((c1 == c2)[same] & (np.abs(w1 - w2)[same] <= 1e-4)) >= 0.999
+
+
+def test_diffusion_tod_and_connectome_within_reference_sampling_noise():
+    """With noise the tracks diverge between any two binary32 implementations (ill-conditioned drift);
+    the distance of the oracle's result from the reference's is below that of two reference runs
+    with different seeds."""
+    from tractography_b200.tracking import contributions_to_matrix
+
+    field, domain, bvh = _cross_case()
+    alg = tg.algorithm.Diffusion(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.1, gamma=1.0,
+                                 noise_variance=0.05)
+    nv = len(domain.boundary.vertices)
+    case = oracle_case(alg, domain, field, rng_seed=99)
+
+    def mat(r):
+        return contributions_to_matrix(*r, nv).toarray()
+
+    A = mat(R.connectome(domain, field, bvh, "diffusion", 0.1, 1.0, 0.05, 99, 20000, 120, 0.5, threads=8))
+    B = mat(R.connectome(domain, field, bvh, "diffusion", 0.1, 1.0, 0.05, 100, 20000, 120, 0.5, threads=8))
+    C = mat(case.connectome(bvh, domain.boundary_arrays(), 20000, 120, 0.5))
+    assert np.abs(A - C).sum() < np.abs(A - B).sum()
+    T1 = R.tod(domain, field, bvh, "diffusion", 0.1, 1.0, 0.05, 99, 20000, 80, (12, 12, 3), np.eye(4), threads=8)
+    T2 = R.tod(domain, field, bvh, "diffusion", 0.1, 1.0, 0.05, 100, 20000, 80, (12, 12, 3), np.eye(4), threads=8)
+    T3 = case.tod(domain.boundary_arrays(), 20000, 80, (12, 12, 3), np.eye(4))
+    assert np.abs(T1 - T3).sum() < np.abs(T1 - T2).sum()

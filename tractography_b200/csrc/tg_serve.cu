@@ -372,8 +372,8 @@ struct ServeRequest {
     int kind = 0;
     tg_job job{};
     TrackParams tp{};
-    std::vector<float> host_seeds;
-    std::vector<uint32_t> host_rng;
+    const float* host_seeds = nullptr;        // caller's, valid until the request finishes
+    const uint32_t* host_rng = nullptr;
     uint32_t n_batches = 0;
     uint64_t reserve = 0;       // bytes counted against the budget while admitted
     // device (admitted)
@@ -498,11 +498,8 @@ int admit(tg_server* S)
         TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&r->d_offset), (size_t)n * 8, S->stream));
         TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&r->d_result), r->result_cap * 12, S->stream));
         // pageable copies are staged before cudaMemcpyAsync returns
-        TG_STRY(cudaMemcpyAsync(r->d_seeds, r->host_seeds.data(), (size_t)n * 32, cudaMemcpyHostToDevice, S->stream));
-        TG_STRY(cudaMemcpyAsync(r->d_rng, r->host_rng.data(), (size_t)r->n_batches * 4, cudaMemcpyHostToDevice,
-                                S->stream));
-        r->host_seeds = std::vector<float>();
-        r->host_rng = std::vector<uint32_t>();
+        TG_STRY(cudaMemcpyAsync(r->d_seeds, r->host_seeds, (size_t)n * 32, cudaMemcpyHostToDevice, S->stream));
+        TG_STRY(cudaMemcpyAsync(r->d_rng, r->host_rng, (size_t)r->n_batches * 4, cudaMemcpyHostToDevice, S->stream));
         ServeJob& J = S->h_jobs[slot];
         std::memset(&J, 0, sizeof J);
         J.t = r->tp;
@@ -744,8 +741,8 @@ int tg_server_submit(tg_server* S, const tg_job* job, uint64_t* request_id)
     r->tp = tp;
     const uint32_t n = job->n_seeds;
     r->n_batches = n ? (n + job->batch_size - 1) / job->batch_size : 0;
-    r->host_seeds.assign(job->seeds, job->seeds + (size_t)n * 8);
-    r->host_rng.assign(job->batch_rng_seeds, job->batch_rng_seeds + r->n_batches);
+    r->host_seeds = job->seeds;
+    r->host_rng = job->batch_rng_seeds;
     r->reserve = (uint64_t)n * 48 + (uint64_t)r->n_batches * 4 +
                  std::max<uint64_t>(1024, (uint64_t)n * std::min<uint64_t>(job->n_steps, S->points_estimate)) * 12;
     r->t_submit = now_s();

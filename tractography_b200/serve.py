@@ -60,6 +60,7 @@ class Server:
             _lib.check(self.lib.tg_server_create(int(hbm_budget_bytes), int(pool_points), int(epoch_steps),
                                                  int(max_requests), ctypes.byref(self._handle)))
         self._jobs = {}
+        self._arrays = {}
         self._ids = (ctypes.c_uint64 * 1024)()
 
     def close(self) -> None:
@@ -97,7 +98,9 @@ class Server:
             s.n_steps = job.n_steps
             rid = ctypes.c_uint64()
             _lib.check(self.lib.tg_server_submit(self._handle, ctypes.byref(s), ctypes.byref(rid)))
+        # the server reads the host seeds at admission: keep them alive until the result is taken
         self._jobs[rid.value] = job
+        self._arrays[rid.value] = (seeds, rng)
         return rid.value
 
     def poll(self) -> list[int]:
@@ -128,6 +131,7 @@ class Server:
                                                offsets.ctypes.data_as(ctypes.c_void_p),
                                                pts.ctypes.data_as(ctypes.c_void_p) if points else None))
         self._jobs.pop(request_id, None)
+        self._arrays.pop(request_id, None)
         return (pts[:p] if points else None), offsets[:n].astype(np.int64), lengths[:n].astype(np.int64), seconds
 
     def result(self, request_id: int) -> Tractogram:
