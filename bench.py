@@ -791,7 +791,7 @@ def run_serve(args):
             arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
             offered = 0
             server = Server(runtime, hbm_budget_bytes=150e9 - resident, pool_points=256 << 20, epoch_steps=1024,
-                            max_requests=512)
+                            max_requests=128)
             latency, seeds_done = [], 0
             t0 = time.perf_counter()
             submitted = 0

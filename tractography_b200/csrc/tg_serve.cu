@@ -405,7 +405,7 @@ struct tg_server {
     uint64_t reserved = 0;
     uint32_t epoch_steps = 1024;
     uint32_t max_slots = 256;
-    uint64_t points_estimate = 64;   // result points per seed assumed at admission
+    uint64_t points_estimate = 160;  // result points per seed assumed at admission
     int sms = 148;
     cudaStream_t stream = nullptr;
     cudaStream_t kstream[kServeKinds] = {};

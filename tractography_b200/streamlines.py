@@ -203,3 +203,107 @@ def load_tck(filename) -> Tractogram:
     if start < len(pts):
         arrays.append(pts[start:])
     return Tractogram(ArraySequence.from_arrays(arrays), affine_to_rasmm=np.eye(4))
+
+
+# ---------------------------------------------------------------------- TRX
+
+class TrxWriter:
+    """Streaming writer of the TRX tractography format (the batch writer of
+    cli/tractogram.py:81-139, which the reference builds on trx-python).
+
+    TRX layout (public format): a ZIP archive, stored uncompressed, holding
+    ``header.json`` (``VOXEL_TO_RASMM`` 4x4, ``DIMENSIONS``, ``NB_VERTICES``,
+    ``NB_STREAMLINES``), ``positions.3.float32`` (all points, little-endian
+    float32 triplets) and ``offsets.uint64`` (index of each streamline's first
+    point).  Batches are appended to spooled files as packed arrays -- the
+    GPU's output layout -- so no per-streamline Python objects are made.
+    """
+
+    def __init__(self, filename, affine=None, dimensions=(1, 1, 1)):
+        import tempfile
+
+        self.filename = Path(filename)
+        self.affine = np.eye(4) if affine is None else np.asarray(affine, dtype=np.float64)
+        self.dimensions = [int(d) for d in dimensions]
+        self._dir = tempfile.TemporaryDirectory()
+        self._pos = open(Path(self._dir.name) / "positions", "wb")
+        self._off = open(Path(self._dir.name) / "offsets", "wb")
+        self.n_vertices = 0
+        self.n_streamlines = 0
+
+    def append(self, points, lengths, offsets=None) -> None:
+        """Append streamlines given as packed points (P, 3) with per-streamline
+        lengths (and offsets into points; default: consecutive)."""
+        points = np.asarray(points, dtype="<f4").reshape(-1, 3)
+        lengths = np.asarray(lengths, dtype=np.int64)
+        if offsets is None:
+            data = points[: int(lengths.sum())]
+        else:
+            offsets = np.asarray(offsets, dtype=np.int64)
+            data = points[np.concatenate([np.arange(o, o + n) for o, n in zip(offsets, lengths)])] \
+                if len(lengths) else points[:0]
+        starts = self.n_vertices + np.concatenate([[0], np.cumsum(lengths)[:-1]]) if len(lengths) else lengths
+        np.ascontiguousarray(data, dtype="<f4").tofile(self._pos)
+        np.asarray(starts, dtype="<u8").tofile(self._off)
+        self.n_vertices += int(lengths.sum())
+        self.n_streamlines += len(lengths)
+
+    def append_tractogram(self, tractogram) -> None:
+        seq = tractogram.streamlines if hasattr(tractogram, "streamlines") else tractogram
+        if isinstance(seq, ArraySequence):
+            self.append(seq.data, seq.lengths, seq.offsets)
+        else:
+            arrays = [np.asarray(s, dtype=np.float32).reshape(-1, 3) for s in seq]
+            self.append(np.concatenate(arrays) if arrays else np.empty((0, 3), np.float32),
+                        np.array([len(a) for a in arrays], dtype=np.int64))
+
+    def close(self) -> None:
+        import json
+        import zipfile
+
+        if self._pos is None:
+            return
+        self._pos.close()
+        self._off.close()
+        header = {"VOXEL_TO_RASMM": self.affine.tolist(), "DIMENSIONS": self.dimensions,
+                  "NB_VERTICES": self.n_vertices, "NB_STREAMLINES": self.n_streamlines}
+        with zipfile.ZipFile(self.filename, "w", compression=zipfile.ZIP_STORED, allowZip64=True) as z:
+            z.writestr("header.json", json.dumps(header))
+            z.write(Path(self._dir.name) / "positions", "positions.3.float32")
+            z.write(Path(self._dir.name) / "offsets", "offsets.uint64")
+        self._pos = None
+        self._dir.cleanup()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def save_trx(filename, tractogram, affine=None, dimensions=(1, 1, 1)) -> None:
+    """Write a Tractogram (or sequence of (n, 3) arrays) as a TRX archive."""
+    with TrxWriter(filename, affine, dimensions) as w:
+        w.append_tractogram(tractogram)
+
+
+def load_trx(filename):
+    """Read a TRX archive written with float32 positions and uint32/uint64
+    offsets; returns (Tractogram, header dict)."""
+    import json
+    import zipfile
+
+    with zipfile.ZipFile(filename) as z:
+        header = json.loads(z.read("header.json"))
+        names = z.namelist()
+        pos_name = next(n for n in names if n.startswith("positions.3."))
+        off_name = next(n for n in names if n.startswith("offsets."))
+        positions = np.frombuffer(z.read(pos_name), dtype="<" + _TRX_DTYPES[pos_name.rsplit(".", 1)[1]]).reshape(-1, 3)
+        offsets = np.frombuffer(z.read(off_name), dtype="<" + _TRX_DTYPES[off_name.rsplit(".", 1)[1]]).astype(np.int64)
+    n = int(header["NB_STREAMLINES"])
+    lengths = np.diff(np.concatenate([offsets[:n], [int(header["NB_VERTICES"])]]))
+    seq = ArraySequence(positions.astype(np.float32), offsets[:n], lengths)
+    return Tractogram(seq, affine_to_rasmm=np.eye(4)), header
+
+
+_TRX_DTYPES = {"float16": "f2", "float32": "f4", "float64": "f8", "uint32": "u4", "uint64": "u8"}
