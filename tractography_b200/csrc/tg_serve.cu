@@ -26,8 +26,12 @@
  *   - a request is admitted when a job slot is free and its buffers fit in
  *     the HBM budget next to the resident objects and the pool; the rest
  *     wait on the host in arrival order;
- *   - a streamline whose pool chunk cannot be allocated is re-queued from
- *     its seed (its partial chunks are released).
+ *   - a streamline starts only after reserving its worst-case number of
+ *     chunks (ceil(n_steps / 32)) against the pool; a seed that finds no room
+ *     is carried, unstarted, to the next epoch, and unused reservations and
+ *     freed chunks are given back, so an allocation never fails and every
+ *     streamline that starts finishes (the overflow re-queue path remains as
+ *     a safety net).
  *
  * A streamline's arithmetic depends only on its seed, its batch's RNG seed
  * and its index in the batch, so every request's result is identical to the
@@ -70,6 +74,7 @@ struct ServeJob {
     uint32_t* lengths;
     int32_t* first_chunk;
     unsigned int* counts;       // [0] streamlines in flight, [1] overflowed
+    uint32_t chunks_needed;     // worst case per streamline: ceil(n_steps / 32)
     unsigned long long* finished_points;   // points of streamlines finished this epoch
     float* result;              // (capacity, 3) harvested points
     uint64_t* result_offset;    // per seed: first point in `result`
@@ -86,6 +91,11 @@ struct ServePool {
     int32_t* chunk_next;
     int32_t* free_list;
     unsigned int* alloc;        // [0] free chunks at the list's head, [1] taken this epoch
+    // chunks held or reserved: a streamline starts only after reserving its
+    // worst case, so an allocation never fails; freed chunks and unused
+    // reservations are given back
+    unsigned long long* committed;
+    uint32_t n_chunks;
 };
 
 struct ServeParams {
@@ -155,22 +165,40 @@ __global__ void __launch_bounds__(128, 5) serve_kernel(const ServeParams sp)
     for (int k = 0; k < CPAD; ++k) c[k] = 0.0f;
     const uint32_t avail = sp.P.alloc[0];
     Lane s;
+    s.px = s.py = s.pz = 0.0f;
     const ServeJob* J = nullptr;
     uint32_t slot = 0, item = 0, fill = 0;
     int32_t chunk = -1;
     uint32_t budget = sp.step_budget;
     unsigned long long steps_total = 0;
 
+    // Reserve the streamline's worst-case chunks, take its first chunk and
+    // write the seed point; false when the pool cannot hold it now.
+    auto start = [&]() -> bool {
+        const unsigned long long W = J->chunks_needed;
+        if (atomicAdd(sp.P.committed, W) + W > (unsigned long long)sp.P.n_chunks) {
+            atomicAdd(sp.P.committed, (unsigned long long)(-(long long)W));
+            return false;
+        }
+        if (!s_alloc(sp.P, avail, chunk)) {             // cannot happen while reservations hold
+            atomicAdd(sp.P.committed, (unsigned long long)(-(long long)W));
+            return false;
+        }
+        J->first_chunk[item] = chunk;
+        fill = 0;
+        s_emit(sp.P, avail, chunk, fill, s.px, s.py, s.pz);
+        return true;
+    };
+
     auto fetch = [&]() -> bool {
-        while (budget > 0u) {
-            const unsigned long long k = atomicAdd(sp.counter, 1ull);
-            if (k < sp.n_carry) {
-                const LaneCarry& cc = sp.carry_in[k];
-                lane_restore(s, cc, item, chunk, fill);
-                slot = cc.job;
-                J = sp.jobs + slot;
-                return true;
-            }
+        if (budget == 0u) return false;
+        const unsigned long long k = atomicAdd(sp.counter, 1ull);
+        if (k < sp.n_carry) {
+            const LaneCarry& cc = sp.carry_in[k];
+            lane_restore(s, cc, item, chunk, fill);
+            slot = cc.job;
+            J = sp.jobs + slot;
+        } else {
             const unsigned long long q0 = k - sp.n_carry;
             if (q0 >= sp.n_new) return false;
             const uint32_t q = seg_upper_bound(sp.seg_prefix, sp.n_seg + 1, (uint32_t)q0) - 1;
@@ -181,19 +209,15 @@ __global__ void __launch_bounds__(128, 5) serve_kernel(const ServeParams sp)
             const float4 b = J->seeds[2 * (size_t)item + 1];
             const uint32_t batch = item / J->batch_size;
             lane_init(s, a, b, J->batch_rng_seeds[batch], item - batch * J->batch_size, J->seed_offset + item);
-            if (!s_alloc(sp.P, avail, chunk)) {
-                J->first_chunk[item] = -1;
-                J->lengths[item] = kOverflowBit;
-                atomicAdd(J->counts + 1, 1u);
-                continue;
-            }
-            J->first_chunk[item] = chunk;
-            fill = 0;
-            s_emit(sp.P, avail, chunk, fill, a.x, a.y, a.z);
             atomicAdd(J->counts, 1u);
-            return true;
+            chunk = -1;
         }
-        return false;
+        if (chunk < 0 && !start()) {
+            // no room in the pool now: hand the unstarted seed to the next epoch
+            lane_save(sp.carry_out + atomicAdd(sp.carry_out_count, 1u), s, item, -1, 0u, slot);
+            return false;
+        }
+        return true;
     };
 
     bool live = fetch();
@@ -224,6 +248,11 @@ __global__ void __launch_bounds__(128, 5) serve_kernel(const ServeParams sp)
         }
         if (done) {
             J->lengths[item] = overflow ? (s.n | kOverflowBit) : s.n;
+            // give back the reservation this streamline will not use (its
+            // chunks are given back when they are freed)
+            const unsigned long long held = ((unsigned long long)s.n + kChunkPoints - 1) / kChunkPoints;
+            const unsigned long long W = J->chunks_needed;
+            atomicAdd(sp.P.committed, (unsigned long long)(-(long long)(W > held ? W - held : 0ull)));
             if (overflow) {
                 atomicAdd(J->counts + 1, 1u);
             } else {
@@ -306,7 +335,8 @@ __global__ void pool_settle_kernel(unsigned int* alloc)
 __global__ void __launch_bounds__(256) harvest_kernel(const ServeJob* __restrict__ jobs,
                                                       const Finished* __restrict__ finished, uint32_t n,
                                                       const float* __restrict__ pool, const int32_t* chunk_next,
-                                                      int32_t* free_list, unsigned int* alloc)
+                                                      int32_t* free_list, unsigned int* alloc,
+                                                      unsigned long long* committed)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -333,7 +363,10 @@ __global__ void __launch_bounds__(256) harvest_kernel(const ServeJob* __restrict
             }
             const int32_t next = chunk_next[chunk];
             __syncwarp();
-            if (lane == 0) free_list[atomicAdd(alloc, 1u)] = chunk;
+            if (lane == 0) {
+                free_list[atomicAdd(alloc, 1u)] = chunk;
+                atomicAdd(committed, (unsigned long long)-1ll);
+            }
             chunk = next;
         }
     }
@@ -341,7 +374,8 @@ __global__ void __launch_bounds__(256) harvest_kernel(const ServeJob* __restrict
 
 // Release the chunks of the listed (overflowed) streamlines and reset them.
 __global__ void release_kernel(const int32_t* chunk_next, int32_t* first_chunk, uint32_t* lengths,
-                               const uint32_t* ids, uint32_t n, int32_t* free_list, unsigned int* alloc)
+                               const uint32_t* ids, uint32_t n, int32_t* free_list, unsigned int* alloc,
+                               unsigned long long* committed)
 {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -350,6 +384,7 @@ __global__ void release_kernel(const int32_t* chunk_next, int32_t* first_chunk, 
     while (chunk >= 0) {
         const int32_t next = chunk_next[chunk];
         free_list[atomicAdd(alloc, 1u)] = chunk;
+        atomicAdd(committed, (unsigned long long)-1ll);
         chunk = next;
     }
     first_chunk[i] = -1;
@@ -515,6 +550,7 @@ int admit(tg_server* S)
         J.cursor = S->d_slot_points + 2 * slot + 1;
         J.result = r->d_result;
         J.result_offset = r->d_offset;
+        J.chunks_needed = (r->job.n_steps + kChunkPoints - 1) / kChunkPoints;
         int st = write_slot(S, slot);
         if (st != TG_OK) return st;
         TG_STRY(cudaMemsetAsync(S->d_counts + 2 * slot, 0, 2 * sizeof(unsigned int), S->stream));
@@ -600,7 +636,8 @@ int requeue_overflow(tg_server* S, int slot)
         TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&d_ids), ids.size() * 4, S->stream));
         TG_STRY(cudaMemcpyAsync(d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, S->stream));
         release_kernel<<<((uint32_t)ids.size() + 127) / 128, 128, 0, S->stream>>>(
-            S->P.chunk_next, r->d_first, r->d_lengths, d_ids, (uint32_t)ids.size(), S->P.free_list, S->P.alloc);
+            S->P.chunk_next, r->d_first, r->d_lengths, d_ids, (uint32_t)ids.size(), S->P.free_list, S->P.alloc,
+            S->P.committed);
         TG_STRY(cudaGetLastError());
         TG_STRY(cudaFreeAsync(d_ids, S->stream));
         size_t a = 0;                            // contiguous runs become queue segments
@@ -666,6 +703,9 @@ int tg_server_create(uint64_t hbm_budget_bytes, uint64_t pool_points, uint32_t e
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->P.chunk_next), chunks * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->P.free_list), chunks * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->P.alloc), 2 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->P.committed), sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(S->P.committed, 0, sizeof(unsigned long long), S->stream);
+    S->P.n_chunks = (uint32_t)chunks;
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->d_carry_count), kServeKinds * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->d_counter), kServeKinds * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->d_steps), sizeof(unsigned long long));
@@ -714,7 +754,7 @@ int tg_server_destroy(tg_server* S)
         if (S->kdone[k]) cudaEventDestroy(S->kdone[k]);
     }
     void* bufs[] = {S->d_jobs, S->d_counts, S->d_slot_points, S->P.pool, S->P.chunk_next, S->P.free_list,
-                    S->P.alloc, S->d_carry_count, S->d_counter, S->d_steps, S->d_segs, S->d_finished,
+                    S->P.alloc, S->P.committed, S->d_carry_count, S->d_counter, S->d_steps, S->d_segs, S->d_finished,
                     S->d_n_finished};
     for (void* b : bufs) cudaFree(b);
     if (S->ev_fork) cudaEventDestroy(S->ev_fork);
@@ -734,6 +774,8 @@ int tg_server_submit(tg_server* S, const tg_job* job, uint64_t* request_id)
     if (job->n_steps == 0) return sfail(TG_ERR_INVALID_ARGUMENT, "n_steps must be positive");
     if (job->n_seeds > 0 && (job->seeds == nullptr || job->batch_rng_seeds == nullptr || job->batch_size == 0))
         return sfail(TG_ERR_INVALID_ARGUMENT, "missing seeds or batch seeds");
+    if ((job->n_steps + kChunkPoints - 1) / kChunkPoints > S->n_chunks)
+        return sfail(TG_ERR_POOL_EXHAUSTED, "the server's point pool cannot hold one streamline of this request");
     ServeRequest* r = new ServeRequest();
     r->id = S->next_id++;
     r->kind = 2 * class_kind(model, lmax, job->algorithm.algorithm) + (tp.domain_kind == kDomainMesh ? 1 : 0);
@@ -915,7 +957,8 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
             uint64_t g = ((uint64_t)n_fin * 32 + 255) / 256;
             if (g > (uint64_t)S->sms * 16) g = (uint64_t)S->sms * 16;
             harvest_kernel<<<(int)g, 256, 0, S->stream>>>(S->d_jobs, S->d_finished, n_fin, S->P.pool,
-                                                          S->P.chunk_next, S->P.free_list, S->P.alloc);
+                                                          S->P.chunk_next, S->P.free_list, S->P.alloc,
+                                                          S->P.committed);
             TG_STRY(cudaGetLastError());
         }
         for (uint32_t slot : order) {
