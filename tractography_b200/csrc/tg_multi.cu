@@ -67,8 +67,16 @@ __device__ __forceinline__ bool m_emit(const MultiParams& mp, int32_t& chunk, ui
 }
 
 // Drain one class: lanes take seeds from the class queue until it is empty.
+// Tracking parameters of the first kSharedJobs jobs of a class are staged in
+// shared memory at kernel start: every step reads ~25 of them (affine rows,
+// step and noise scales, limits), and lanes of one warp usually follow
+// several jobs, which in the job table in global memory costs one L1
+// wavefront per distinct job per load.
+constexpr int kSharedJobs = 48;
+
 template <int MODEL, int LMAX, int ALGO>
-__device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp, const ClassDev& cls)
+__device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp, const ClassDev& cls,
+                                                          const TrackParams* shared_t, uint32_t n_shared)
 {
     constexpr int CPAD = ModelShape<MODEL, LMAX>::CPAD;
     float c[CPAD];
@@ -76,6 +84,7 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
     for (int k = 0; k < CPAD; ++k) c[k] = 0.0f;
     unsigned long long steps_total = 0;
     const JobDev* J = nullptr;
+    const TrackParams* P = nullptr;
     Lane s;
     int32_t chunk = -1;
     uint32_t fill = 0;
@@ -90,6 +99,7 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
             if (mp.carry_in != nullptr) {
                 lane_restore(s, mp.carry_in[k], g, chunk, fill);
                 J = mp.jobs + (upper_bound_u32(mp.job_base, mp.n_jobs + 1, g) - 1);
+                P = &J->t;
                 return true;
             }
             uint32_t job, i;
@@ -97,13 +107,16 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
                 g = cls.item_ids[k];
                 job = upper_bound_u32(mp.job_base, mp.n_jobs + 1, g) - 1;
                 i = g - mp.job_base[job];
+                J = mp.jobs + job;
+                P = &J->t;
             } else {
                 const uint32_t q = upper_bound_u32(cls.prefix, cls.n_jobs + 1, (uint32_t)k) - 1;
                 job = cls.jobs[q];
                 i = (uint32_t)k - cls.prefix[q];
                 g = mp.job_base[job] + i;
+                J = mp.jobs + job;
+                P = q < n_shared ? shared_t + q : &J->t;
             }
-            J = mp.jobs + job;
             const float4 a = J->seeds[2 * (size_t)i];
             const float4 b = J->seeds[2 * (size_t)i + 1];
             const uint32_t batch = i / J->batch_size;
@@ -130,11 +143,11 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
             break;
         }
         if (!live) continue;
-        bool done = s.n >= J->t.n_steps;
+        bool done = s.n >= P->n_steps;
         bool overflow = false;
         if (!done) {
             float qx, qy, qz;
-            const int r = track_step<MODEL, LMAX, ALGO, CPAD>(J->t, s, c, qx, qy, qz);
+            const int r = track_step<MODEL, LMAX, ALGO, CPAD>(*P, s, c, qx, qy, qz);
             if (r == 0) {
                 done = true;
             } else if (r == 2) {
@@ -158,15 +171,32 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
 template <int MODEL, int LMAX, int ALGO>
 __global__ void __launch_bounds__(128, 5) track_class_kernel(const MultiParams mp, const ClassDev cls)
 {
-    const unsigned long long steps = drain_class<MODEL, LMAX, ALGO>(mp, cls);
+    extern __shared__ uint4 shared_raw[];
+    TrackParams* table = reinterpret_cast<TrackParams*>(shared_raw);
+    const uint32_t n_shared = cls.n_jobs < (uint32_t)kSharedJobs ? cls.n_jobs : (uint32_t)kSharedJobs;
+    constexpr uint32_t kWords = sizeof(TrackParams) / sizeof(uint32_t);
+    static_assert(sizeof(TrackParams) % sizeof(uint32_t) == 0, "TrackParams is copied as words");
+    for (uint32_t w = threadIdx.x; w < n_shared * kWords; w += blockDim.x) {
+        const uint32_t q = w / kWords, o = w - q * kWords;
+        reinterpret_cast<uint32_t*>(table + q)[o] =
+            reinterpret_cast<const uint32_t*>(&mp.jobs[cls.jobs[q]].t)[o];
+    }
+    __syncthreads();
+    const unsigned long long steps = drain_class<MODEL, LMAX, ALGO>(mp, cls, table, n_shared);
     if (steps != 0) atomicAdd(mp.steps_done, steps);
+}
+
+size_t class_shared_bytes(uint32_t n_jobs)
+{
+    const uint32_t n = n_jobs < (uint32_t)kSharedJobs ? n_jobs : (uint32_t)kSharedJobs;
+    return (size_t)n * sizeof(TrackParams);
 }
 
 template <int M, int L, int A>
 struct ClassLaunch {
     static cudaError_t run(const MultiParams& mp, const ClassDev& cls, int grid, cudaStream_t stream)
     {
-        track_class_kernel<M, L, A><<<grid, 128, 0, stream>>>(mp, cls);
+        track_class_kernel<M, L, A><<<grid, 128, class_shared_bytes(cls.n_jobs), stream>>>(mp, cls);
         return cudaGetLastError();
     }
 };
@@ -175,7 +205,8 @@ template <int M, int L, int A>
 struct ClassOccupancy {
     static cudaError_t run(int* blocks)
     {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, track_class_kernel<M, L, A>, 128, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, track_class_kernel<M, L, A>, 128,
+                                                             class_shared_bytes(kSharedJobs));
     }
 };
 
