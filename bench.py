@@ -167,6 +167,24 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def combine_ranks(dist, times, counts, device):
+    """Whole-job figures of independent replicas: the slowest rank's times
+    (max) and the work of all ranks (sum).  No data-path collective: the
+    ranks track disjoint seed sets and only these scalars are exchanged."""
+    import torch
+
+    t = torch.tensor(times, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor(counts, dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return [float(x) for x in t.tolist()], [int(x) for x in c.tolist()]
+
+
+def replica_seed(rank: int) -> int:
+    """NumPy seed of a replica's seeds.from_fod draw (distinct per rank)."""
+    return 2024 + rank
+
+
 def setup_workload(rank: int, n_seeds: int, runtime):
     import tractography_b200 as tg
     from tractography_b200 import synthetic
@@ -176,7 +194,7 @@ def setup_workload(rank: int, n_seeds: int, runtime):
     mask = np.any(field.values != 0, axis=-1).astype(np.uint8)
     domain = tg.domain.Image(tg.Nifti1Image(mask, fod.affine))
     state = np.random.get_state()
-    np.random.seed(2024 + rank)
+    np.random.seed(replica_seed(rank))
     try:
         seeds = tg.seeds.from_fod(fod, n_seeds, runtime=runtime)
     finally:
@@ -290,12 +308,8 @@ def run_ours(args):
                 dist.barrier()
 
     if dist is not None:
-        t = torch.tensor([dev_ms, e2e_ms, kernel_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        c = torch.tensor([dev_steps, e2e_steps, dev_points, n_launch, n_waves], dtype=torch.float64, device="cuda")
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        dev_ms, e2e_ms, kernel_ms = (float(x) for x in t.tolist())
-        dev_steps, e2e_steps, dev_points, n_launch, n_waves = (int(x) for x in c.tolist())
+        (dev_ms, e2e_ms, kernel_ms), (dev_steps, e2e_steps, dev_points, n_launch, n_waves) = combine_ranks(
+            dist, [dev_ms, e2e_ms, kernel_ms], [dev_steps, e2e_steps, dev_points, n_launch, n_waves], "cuda")
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
