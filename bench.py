@@ -94,6 +94,26 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def profile_constant(key):
+    """A per-step constant recorded in the committed ncu summary of the tracking kernel."""
+    path = ROOT / "profiles" / "track_persistent_config1.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith(key + ":"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+def fp32_peak_tflops():
+    """FP32 FMA peak from the device properties: SMs x 128 lanes x 2 FLOP x SM clock."""
+    import torch
+
+    props = torch.cuda.get_device_properties(0)
+    clock_khz = getattr(props, "clock_rate", 0) or 1965000
+    return props.multi_processor_count * 128 * 2 * clock_khz * 1e3 / 1e12
+
+
 def traffic_per_step():
     """DRAM bytes per accepted step of the tracking kernel from the committed ncu summary."""
     path = ROOT / "profiles" / "track_persistent_config1.md"
@@ -364,6 +384,14 @@ def run_ours(args):
         },
         "clocks": sampler.summary(),
     }
+    flop = profile_constant("fp32_flop_per_step")
+    if flop is not None:
+        tflops = kernel_steps_per_s * flop / 1e12
+        peak_fp32 = fp32_peak_tflops()
+        line["fp32"] = {"flop_per_step": flop, "achieved_tflops": tflops, "peak_tflops": peak_fp32,
+                        "frac": tflops / peak_fp32,
+                        "note": "FP32 FLOP per step from the ncu instruction mix of the tracking kernel "
+                                "(FFMA = 2); peak = SMs x 128 x 2 x SM clock"}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(field, domain, seeds)
     print(json.dumps(line), flush=True)
