@@ -53,3 +53,11 @@ def test_invalid_arguments_fail_without_a_device():
     assert b"null" in lib.tg_last_error()
     with pytest.raises(ValueError):
         _lib.check(status)
+
+
+def test_missing_library_fails_loudly(tmp_path, monkeypatch):
+    """No CPU fallback: without libtg_b200.so the package raises instead of tracking on the host."""
+    monkeypatch.setattr(_lib, "LIB_PATH", tmp_path / "absent.so")
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(RuntimeError, match="not built"):
+        _lib.load()
