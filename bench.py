@@ -849,8 +849,12 @@ def run_serve(args):
                     _, _, lengths, seconds = server.take(rid, points=False)
                     latency.append(seconds)
                     seeds_done += len(lengths)
-                if not finished and server.active == 0 and server.pending == 0 and submitted < n_req:
+                if not finished and server.active == 0 and server.pending == 0:
+                    if submitted == n_req:
+                        raise RuntimeError("the server holds no work but requests are unfinished")
                     time.sleep(max(0.0, min(0.002, arrivals[submitted] - (time.perf_counter() - t0))))
+                if time.perf_counter() - t0 > 600.0:
+                    raise RuntimeError(f"rate {rate}: requests still unfinished after 600 s")
             wall = time.perf_counter() - t0
             st = server.stats()
             server.close()
