@@ -76,9 +76,12 @@ def test_requests_equal_alone_in_the_mix(runtime, epoch_steps, pool_points):
         for _ in range(3 if w < 2 else 0):          # later waves arrive while earlier requests run
             for rid in server.poll():
                 results[rid] = server.take(rid)
+    polls = 0
     while len(results) < len(jobs):
         for rid in server.poll():
             results[rid] = server.take(rid)
+        polls += 1
+        assert polls < 20000, "requests stopped making progress"
     stats = server.stats()
     server.close()
     for rid, (points, offsets, lengths, seconds) in results.items():

@@ -152,7 +152,11 @@ class Server:
         """Poll until every submitted request finished; returns {id: Tractogram}."""
         out = {}
         idle = 0
+        polls = 0
         while self._jobs:
+            polls += 1
+            if polls > 10_000_000:
+                raise RuntimeError("requests stopped making progress")
             finished = self.poll()
             for rid in finished:
                 out[rid] = self.result(rid)
