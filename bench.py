@@ -77,7 +77,7 @@ def parse_args():
     p.add_argument("--seeds", type=int, default=1000000, help="seeds per step (one tg.tractogram job)")
     p.add_argument("--batch", type=int, default=50000, help="reference batch_size inside a job")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["config1", "mixed", "config2", "serve"], default="config1",
+    p.add_argument("--workload", choices=["config1", "config0", "mixed", "config2", "serve"], default="config1",
                    help="config1 (default headline), the 64-job mixed workload, the DTI + mesh workload, or "
                         "serving under Poisson load")
     p.add_argument("--rates", default="5,20,50,100,200", help="serving: arrival rates (requests/s)")
@@ -628,6 +628,100 @@ def run_mixed(args):
     print(json.dumps(line), flush=True)
 
 
+C0_WORKLOAD = ("config0 Transport: SH lmax 8 (45 f32 coefficients) 32^3 at 2 mm, bundle along x and y-z arcs, "
+               "ellipsoid mask 14/12/12 voxels; 10000 seeds uniform in the mask; step 0.2 mm (0.1 voxel), gamma 1; "
+               "save_at 0.25, max length 300 mm")
+
+
+def run_config0(args):
+    """Config 0: the reference's CPU-runnable Transport case, GPU vs the reference kernel on the host."""
+    import torch
+
+    import tractography_b200 as tg
+    from tractography_b200 import _lib, synthetic
+    from tractography_b200.algorithm import to_struct
+
+    torch.cuda.set_device(0)
+    runtime = tg.CudaRuntime(0)
+    lib = runtime.lib
+    sh = ctypes.c_void_p(runtime.stream_handle)
+    fod, mask = synthetic.config0()
+    field, domain = tg.field.Image(fod), tg.domain.Image(mask)
+    n_job = args.seeds if args.seeds != 1000000 else 10000
+    seeds = synthetic.seeds_in_mask(mask, n_job, seed=0)
+    algorithm = tg.algorithm.Transport(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.2, gamma=1.0)
+    n_steps = int(math.floor(MAX_LENGTH / SAVE_AT))
+    rng = np.zeros((n_job + args.batch - 1) // args.batch, np.uint32)
+    with runtime.device_scope():
+        d_h, f_h = domain.device(runtime), field.device(runtime, _lib.MODEL_SH)
+        a = to_struct(algorithm)
+        dev_seeds = runtime.to_device(seeds)
+        lengths = np.empty(n_job, np.uint32)
+        offsets = np.empty(n_job, np.uint64)
+        total, steps = ctypes.c_uint64(), ctypes.c_uint64()
+        kms, waves, launches = ctypes.c_float(), ctypes.c_uint32(), ctypes.c_uint32()
+
+        def run():
+            _lib.check(lib.tg_tracker_run(runtime.tracker(), ctypes.byref(a), d_h, f_h,
+                                          ctypes.c_void_p(dev_seeds.data_ptr()), 0, n_job, args.batch,
+                                          rng.ctypes.data_as(ctypes.c_void_p), SAVE_AT, n_steps,
+                                          lengths.ctypes.data_as(ctypes.c_void_p),
+                                          offsets.ctypes.data_as(ctypes.c_void_p), ctypes.byref(total),
+                                          ctypes.byref(steps), sh))
+            _lib.check(lib.tg_tracker_stats(runtime.tracker(), ctypes.byref(kms), ctypes.byref(waves),
+                                            ctypes.byref(launches)))
+            return int(steps.value), float(kms.value), int(launches.value)
+
+        for _ in range(args.warmup):
+            run()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(0)
+        with sampler:
+            torch.cuda.synchronize()
+            ev0.record(runtime.stream)
+            dev_steps = n_launch = 0
+            kernel_ms = 0.0
+            for _ in range(args.steps):
+                st, k, nl = run()
+                dev_steps, kernel_ms, n_launch = dev_steps + st, kernel_ms + k, n_launch + nl
+            ev1.record(runtime.stream)
+            torch.cuda.synchronize()
+            dev_ms = ev0.elapsed_time(ev1)
+    peak, peak_kind = measured_peaks()
+    bps = 4 * 45 + 4 + 16 * 0.2 / SAVE_AT
+    kernel_sps = dev_steps / (kernel_ms / 1e3)
+    line = {"metric": METRIC, "value": dev_steps / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator; no dataset)",
+            "workload": "config0",
+            "config": {"workload": C0_WORKLOAD, "seeds_per_step": n_job,
+                       "cache": "volume (5.9 MB) L2-resident; one job is far below one GPU's lanes"},
+            "streamlines_per_s": n_job * args.steps / (dev_ms / 1e3), "gpu_launches": n_launch,
+            "roofline": {"bound": "hbm", "achieved": kernel_sps * bps / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": kernel_sps * bps / 1e9 / peak, "bytes_per_step": bps,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+            "clocks": sampler.summary()}
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        ref = _reference_lib()
+        t0 = time.perf_counter()
+        if ref is not None:
+            st = ref.tractogram_steps(domain, field, "transport", 0.2, 1.0, 0.0, seeds, 0, SAVE_AT, n_steps, threads)
+            kind, what = "reference", "reference OpenCL kernel source compiled as C++ (oracle/_ref)"
+        else:
+            from oracle import oracle as O
+
+            case = O.Case(mask=domain.values, mask_inv_affine=domain.inverse_affine, field=field.values,
+                          field_inv_affine=field.inverse_affine, step_size=0.2, gamma=1.0, save_at=SAVE_AT,
+                          n_steps=n_steps)
+            st = case.tractogram(seeds, n_threads=threads, return_steps=True)[2]
+            kind, what = "port", "plain-C oracle"
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": st / dt, "unit": UNIT, "cores": threads, "kind": kind,
+                                "sample": f"all {n_job} seeds ({st} steps, {dt:.1f} s); {what}, OpenMP over seeds"}
+    print(json.dumps(line), flush=True)
+
+
 C2_STEP = 0.2           # 0.1 voxel at 2 mm
 C2_SEEDS = 2_000_000
 C2_BYTES_PER_STEP = 4 * 6 + 1 + 16 * C2_STEP / SAVE_AT
@@ -885,6 +979,8 @@ def main():
         run_mixed(args)
     elif args.workload == "config2":
         run_config2(args)
+    elif args.workload == "config0":
+        run_config0(args)
     elif args.workload == "serve":
         run_serve(args)
     else:
