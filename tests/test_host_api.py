@@ -227,6 +227,43 @@ def test_tck_round_trip(tmp_path):
         np.testing.assert_array_equal(a, b)
 
 
+def test_tck_writer_streams_packed_batches(tmp_path):
+    """Batches appended as packed (points, lengths, offsets) give the same bytes
+    as one save_tck of the whole set, non-consecutive offsets included."""
+    rng = np.random.default_rng(1)
+    lengths = rng.integers(1, 30, 200)
+    arrays = [rng.normal(size=(n, 3)).astype(np.float32) for n in lengths]
+    whole = tmp_path / "whole.tck"
+    tg.save_tck(whole, tg.Tractogram(arrays, affine_to_rasmm=np.eye(4)))
+    streamed = tmp_path / "streamed.tck"
+    with tg.TckWriter(streamed) as w:
+        for lo in range(0, 200, 64):
+            part = arrays[lo: lo + 64]
+            # packed with a gap before each streamline and a fourth column, as the GPU layout has
+            gap = 2
+            offsets = np.cumsum([0] + [len(a) + gap for a in part])[:-1] + gap
+            pts = np.full((int(offsets[-1]) + len(part[-1]) + 3, 4), 7.0, np.float32)
+            for o, a in zip(offsets, part):
+                pts[o: o + len(a), :3] = a
+            w.append(pts, [len(a) for a in part], offsets)
+        w.append(np.empty((0, 3), np.float32), [])
+    assert streamed.read_bytes() == whole.read_bytes()
+    back = tg.load_tck(streamed)
+    assert len(back.streamlines) == 200
+    for a, b in zip(arrays, back.streamlines):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_tck_writer_applies_affine(tmp_path):
+    a = np.array([[1, 2, 3], [4, 5, 6]], np.float32)
+    affine = np.diag([2.0, 2.0, 2.0, 1.0])
+    affine[:3, 3] = [1, 0, -1]
+    path = tmp_path / "a.tck"
+    tg.save_tck(path, tg.Tractogram([a], affine_to_rasmm=affine))
+    back = tg.load_tck(path).streamlines[0]
+    np.testing.assert_array_equal(back, a * 2 + np.array([1, 0, -1], np.float32))
+
+
 def test_seed_files_round_trip(tmp_path):
     """seeds.py:243-303"""
     np.random.seed(0)

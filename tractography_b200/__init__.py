@@ -19,7 +19,7 @@ from . import seeds
 from .nifti import Nifti1Image
 from .opencl import BufferAccess, OpenCLRuntime
 from .runtime import CudaRuntime
-from .streamlines import ArraySequence, Tractogram, TrxWriter, load_tck, load_trx, save_tck, save_trx
+from .streamlines import ArraySequence, TckWriter, Tractogram, TrxWriter, load_tck, load_trx, save_tck, save_trx
 
 algorithm = algorithm_module
 domain = domain_module
@@ -27,7 +27,7 @@ field = field_module
 seeds_module = seeds
 
 __all__ = [
-    "ArraySequence", "BufferAccess", "CudaRuntime", "Nifti1Image", "OpenCLRuntime", "Tractogram", "TrxWriter",
+    "ArraySequence", "BufferAccess", "CudaRuntime", "Nifti1Image", "OpenCLRuntime", "TckWriter", "Tractogram", "TrxWriter",
     "load_trx", "save_trx",
     "algorithm", "core", "domain", "field", "jobs", "load_tck", "local", "nifti", "save_tck", "seeds",
     "connectome", "streamlines", "tod", "tracking", "tractogram", "utils",

@@ -136,43 +136,101 @@ def to_nibabel(tractogram: Tractogram):  # pragma: no cover - needs nibabel
 _TCK_MAGIC = b"mrtrix tracks\n"
 
 
+def _packed_rows(points, lengths, offsets):
+    """Rows of packed streamlines laid end to end, each followed by a NaN row.
+
+    ``points`` is (P, 3); streamline i is points[offsets[i] : offsets[i] +
+    lengths[i]] (consecutive when ``offsets`` is None).  One gather, no
+    per-streamline Python work.
+    """
+    lengths = np.asarray(lengths, dtype=np.int64)
+    n = len(lengths)
+    total = int(lengths.sum())
+    out = np.empty((total + n, 3), dtype="<f4")
+    if n == 0:
+        return out
+    ends = np.cumsum(lengths + 1)                   # one past each NaN row
+    starts = ends - lengths - 1                     # first output row of each streamline
+    src0 = np.cumsum(lengths) - lengths if offsets is None else np.asarray(offsets, dtype=np.int64)
+    # output row r of streamline i takes points[src0[i] + (r - starts[i])]
+    rows = np.arange(total, dtype=np.int64) + np.repeat(starts - (np.cumsum(lengths) - lengths), lengths)
+    src = np.repeat(src0 - (np.cumsum(lengths) - lengths), lengths) + np.arange(total, dtype=np.int64)
+    out[rows] = np.asarray(points, dtype=np.float32).reshape(-1, 3)[src]
+    out[ends - 1] = np.nan
+    return out
+
+
+class TckWriter:
+    """Streaming writer of MRtrix ``.tck`` files from packed batches.
+
+    The reference writes through nibabel's ``TckFile`` from a Python list of
+    streamlines (tractography/cli/tractogram.py:68-78).  Here each batch is
+    appended as the packed (points, lengths, offsets) arrays the GPU produces;
+    the header's ``count`` field has a fixed width and is rewritten on
+    ``close``, so the file is written in one pass and no per-streamline
+    Python objects are made.  ``affine`` (voxel-to-RAS, default identity) is
+    applied to every point before it is written.
+    """
+
+    def __init__(self, filename, affine=None):
+        self.filename = Path(filename)
+        self.affine = None if affine is None or np.array_equal(affine, np.eye(4)) else \
+            np.asarray(affine, dtype=np.float64)
+        self.n_streamlines = 0
+        self._f = open(self.filename, "wb")
+        self._f.write(self._header(0))
+
+    @staticmethod
+    def _header(count: int) -> bytes:
+        body = b"count: %010d\n" % count + b"datatype: Float32LE\n"
+        # The offset line's own length depends on the offset: iterate to a fix point.
+        offset = len(_TCK_MAGIC) + len(body) + len(b"file: . 0\nEND\n")
+        while True:
+            total = len(_TCK_MAGIC) + len(body) + len(b"file: . %d\n" % offset) + len(b"END\n")
+            if total <= offset:
+                break
+            offset = total
+        header = _TCK_MAGIC + body + (b"file: . %d\n" % offset) + b"END\n"
+        return header + b" " * (offset - len(header))
+
+    def append(self, points, lengths, offsets=None) -> None:
+        """Append streamlines given as packed points (P, 3) (or (P, 4); the
+        fourth column is dropped) with per-streamline lengths and optional
+        offsets into points (default: consecutive)."""
+        points = np.asarray(points, dtype=np.float32)
+        points = points.reshape(-1, points.shape[-1])[:, :3] if points.size else points.reshape(0, 3)
+        out = _packed_rows(points, lengths, offsets)
+        if self.affine is not None and len(out):
+            out = (out.astype(np.float64) @ self.affine[:3, :3].T + self.affine[:3, 3]).astype("<f4")
+        self._f.write(out.tobytes())
+        self.n_streamlines += len(lengths)
+
+    def append_tractogram(self, tractogram) -> None:
+        seq = tractogram.streamlines if hasattr(tractogram, "streamlines") else tractogram
+        if not isinstance(seq, ArraySequence):
+            seq = ArraySequence.from_arrays(list(seq))
+        self.append(seq.data, seq.lengths, seq.offsets)
+
+    def close(self) -> None:
+        if self._f is None:
+            return
+        self._f.write(np.full((1, 3), np.inf, dtype="<f4").tobytes())
+        self._f.seek(0)
+        self._f.write(self._header(self.n_streamlines))
+        self._f.close()
+        self._f = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def save_tck(filename, tractogram) -> None:
     """Write streamlines (RAS+ mm) to an MRtrix ``.tck`` file."""
-    streamlines = tractogram.streamlines if hasattr(tractogram, "streamlines") else tractogram
-    if not isinstance(streamlines, ArraySequence):
-        streamlines = ArraySequence.from_arrays(list(streamlines))
-    affine = getattr(tractogram, "affine_to_rasmm", None)
-    n = len(streamlines)
-    header_fields = [
-        b"count: %010d\n" % n,
-        b"datatype: Float32LE\n",
-    ]
-    body = b"".join(header_fields)
-    # The offset line's own length depends on the offset: iterate to a fix point.
-    offset = len(_TCK_MAGIC) + len(body) + len(b"file: . 0\nEND\n")
-    while True:
-        line = b"file: . %d\n" % offset
-        total = len(_TCK_MAGIC) + len(body) + len(line) + len(b"END\n")
-        if total <= offset:
-            break
-        offset = total
-    header = _TCK_MAGIC + body + (b"file: . %d\n" % offset) + b"END\n"
-    header = header + b" " * (offset - len(header))
-    lengths = streamlines.lengths
-    out = np.empty((int(lengths.sum()) + n + 1, 3), dtype="<f4")
-    pos = 0
-    for i in range(n):
-        pts = streamlines[i]
-        if affine is not None and not np.array_equal(affine, np.eye(4)):
-            pts = pts @ affine[:3, :3].T + affine[:3, 3]
-        out[pos: pos + len(pts)] = pts
-        pos += len(pts)
-        out[pos] = np.nan
-        pos += 1
-    out[pos] = np.inf
-    with open(filename, "wb") as f:
-        f.write(header)
-        f.write(out.tobytes())
+    with TckWriter(filename, getattr(tractogram, "affine_to_rasmm", None)) as w:
+        w.append_tractogram(tractogram)
 
 
 def load_tck(filename) -> Tractogram:
