@@ -276,3 +276,18 @@ def test_seed_files_round_trip(tmp_path):
         np.testing.assert_allclose(back, s, atol=1e-5)
     with pytest.raises(ValueError, match="Unknown file type"):
         tg.seeds.save(tmp_path / "x.vtk", s)
+
+
+def test_write_tractogram_without_seeds(tmp_path):
+    from tractography_b200 import synthetic
+
+    fod, mask = synthetic.config0(n=8)
+    for suffix in (".tck", ".trx"):
+        path = tmp_path / f"empty{suffix}"
+        assert tg.write_tractogram(path, fod, np.empty((0, 8), np.float32), mask) == 0
+        back = tg.load_tck(path) if suffix == ".tck" else tg.load_trx(path)[0]
+        assert len(back.streamlines) == 0
+    with pytest.raises(ValueError, match="Unknown tractogram file type"):
+        tg.write_tractogram(tmp_path / "x.vtk", fod, np.empty((0, 8), np.float32), mask)
+    with pytest.raises(ValueError, match="save_at must be finite and positive"):
+        tg.write_tractogram(tmp_path / "x.tck", fod, np.empty((0, 8), np.float32), mask, save_at=0.0)

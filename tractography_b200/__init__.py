@@ -30,7 +30,7 @@ __all__ = [
     "ArraySequence", "BufferAccess", "CudaRuntime", "Nifti1Image", "OpenCLRuntime", "TckWriter", "Tractogram", "TrxWriter",
     "load_trx", "save_trx",
     "algorithm", "core", "domain", "field", "jobs", "load_tck", "local", "nifti", "save_tck", "seeds",
-    "connectome", "streamlines", "tod", "tracking", "tractogram", "utils",
+    "connectome", "streamlines", "tod", "tracking", "tractogram", "utils", "write_tractogram",
 ]
 
 
@@ -206,6 +206,42 @@ def tod(field, n_seeds: int = 1000000, domain=None, algorithm=None, *, maximum_s
         tracking_domain = domain_module.Image(domain_image)
     return tracking.tod(tracking_algorithm, tracking_domain, tracking_field, image_grid, n_seeds,
                         maximum_streamline_length=maximum_streamline_length, runtime=runtime)
+
+
+def write_tractogram(
+    filename,
+    field,
+    seeds,
+    domain=None,
+    algorithm=None,
+    *,
+    save_at: float = 1.0,
+    maximum_streamline_length: float = 300.0,
+    minimum_streamline_length: float = 0.0,
+    batch_size: int = 50000,
+    seeds_per_pass: int = 1000000,
+    runtime=None,
+) -> int:
+    """Track like :func:`tractogram` and stream the result to ``filename``
+    (``.tck`` or ``.trx``, by suffix) without building it in memory; the
+    batch writer of tractography/cli/tractogram.py:81-139.  Same arguments,
+    validation and results as :func:`tractogram`; returns the number of
+    streamlines written."""
+    job = jobs.prepare(field, seeds, domain, algorithm, save_at=save_at,
+                       maximum_streamline_length=maximum_streamline_length,
+                       minimum_streamline_length=minimum_streamline_length, batch_size=batch_size,
+                       runtime=runtime)
+    if isinstance(job, Tractogram):
+        from .streamlines import TckWriter, TrxWriter
+
+        suffix = str(filename).lower().rsplit(".", 1)[-1]
+        if suffix not in ("tck", "trx"):
+            raise ValueError(f"Unknown tractogram file type: .{suffix}")
+        (TckWriter if suffix == "tck" else TrxWriter)(filename).close()
+        return 0
+    from .runtime import default_runtime
+
+    return jobs.write(job, filename, runtime or default_runtime(), seeds_per_pass)
 
 
 def tractogram(

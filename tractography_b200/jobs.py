@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass, field as dc_field
+from pathlib import Path
 
 import numpy as np
 
@@ -152,6 +153,45 @@ def run(job: Job, runtime) -> Tractogram:
                                    batch_rng_seeds=job.batch_rng_seeds, runtime=runtime,
                                    philox_key=job.philox_key)
     return _to_tractogram(job, result)
+
+
+def write(job: Job, filename, runtime, seeds_per_pass: int = 1_000_000, affine=None) -> int:
+    """Track a prepared job and stream its streamlines to a ``.tck`` or
+    ``.trx`` file; returns the number of streamlines written.
+
+    The reference's command line does this for TRX by calling
+    ``tracking.tractogram`` per batch and appending the kept streamlines to a
+    memory-mapped writer (tractography/cli/tractogram.py:81-139).  Here the
+    seeds go to the tracker ``seeds_per_pass`` at a time (rounded to whole
+    batches, so every batch keeps its RNG seed and per-batch stream ids) and
+    each pass's packed output is appended to the streaming writer with the
+    minimum-length filter applied as a mask: host memory stays bounded by
+    one pass and no per-streamline Python objects are made.  The file holds
+    exactly the streamlines ``run`` returns, in the same order.
+    """
+    from .streamlines import TckWriter, TrxWriter
+
+    suffix = Path(filename).suffix.lower()
+    if suffix == ".tck":
+        writer = TckWriter(filename, affine)
+    elif suffix == ".trx":
+        writer = TrxWriter(filename, affine)
+    else:
+        raise ValueError(f"Unknown tractogram file type: {suffix or filename}")
+    per_pass = max(1, int(seeds_per_pass) // job.batch_size) * job.batch_size
+    written = 0
+    with writer:
+        for lo in range(0, job.n_seeds, per_pass):
+            hi = min(job.n_seeds, lo + per_pass)
+            b0, b1 = lo // job.batch_size, (hi + job.batch_size - 1) // job.batch_size
+            result = tracking.track_packed(job.algorithm, job.domain, job.field, job.seeds[lo:hi],
+                                           save_at=job.save_at, n_steps=job.n_steps, batch_size=job.batch_size,
+                                           batch_rng_seeds=job.batch_rng_seeds[b0:b1], runtime=runtime,
+                                           philox_key=job.philox_key, seed_offset=lo)
+            keep = result.lengths > job.min_points
+            writer.append(result.points, result.lengths[keep], result.offsets[keep])
+            written += int(keep.sum())
+    return written
 
 
 class JobsResult:
