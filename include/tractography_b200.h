@@ -133,6 +133,14 @@ int tg_mesh_info(const tg_domain* domain, uint32_t* n_triangles, uint32_t* n_nod
 int tg_mesh_segment_hits(const tg_domain* domain, const float* starts, const float* ends, uint32_t n,
                          uint8_t* found, uint32_t* triangle, float* hit, void* stream);
 
+/* The closed-surface domain test of tracking, per segment: blocked[i] = 1
+ * when the segment starts[i] -> ends[i] hits the surface (the found flag of
+ * bvh_segment_hit, utils/bvh.cl:83-131), computed as the tracking kernels
+ * compute it (distance grid, per-cell leaf lists, walk).  Device arrays:
+ * starts/ends (n, 4) float32, blocked (n) uint8. */
+int tg_mesh_segments_blocked(const tg_domain* domain, const float* starts, const float* ends, uint32_t n,
+                             uint8_t* blocked, void* stream);
+
 /* The reference kernel contract (tracking.py:93-176): one launch over
  * n_seeds device seeds; writes the dense (n_seeds, n_steps, 4) float32
  * points and uint32 lengths to device memory exactly as the reference's

@@ -3,8 +3,9 @@
 * segment hits through the C ABI equal the reference's bvh_segment_hit
   (tests/golden/bvh_reference.npz) bit for bit: found flag, triangle,
   barycentric coordinates and t;
-* on the config-2 surface shape, segment hits and the inside test equal the
-  oracle's bit for bit;
+* on the config-2 surface shape, segment hits, the tracking kernels'
+  surface test (distance grid, per-cell leaf lists, walk) and the inside
+  test equal the oracle's bit for bit;
 * tracking with a mesh domain (dense one-thread-per-seed and packed
   persistent forms) equals the oracle's tracking loop bit for bit; the
   oracle walks the BVH for every step while the kernels skip the walk in
@@ -61,6 +62,35 @@ def test_segment_hits_match_oracle_on_config2_surface(runtime):
     assert np.array_equal(got[1], want[1])
     assert bits_equal(got[2], want[2])
     assert 0.1 < got[0].mean() < 0.9
+
+
+@pytest.mark.parametrize("frequency", [40, 158])
+def test_segments_blocked_match_oracle(runtime, frequency):
+    """The tracking kernels' surface test (distance grid, per-cell leaf
+    lists, walk) equals the found flag of the oracle's bvh_segment_hit walk
+    on short segments near the surface (the leaf-list route), longer ones
+    (the walk), far ones (the distance grid), segments from vertices and
+    axis-parallel ones."""
+    v, f = _surface(frequency=frequency)
+    mesh = tg.domain.Mesh(v, f)
+    bvh = O.BoundaryBvh.build(v, f)
+    cell = 192.0 / (min(256, int(np.ceil(0.5 * np.sqrt(len(f))))) - 4)    # about the grid's cell
+    rng = np.random.default_rng(frequency)
+    lo, hi = v.min(axis=0), v.max(axis=0)
+    n = 60000
+    k = rng.integers(0, len(f), n)
+    p = v[f[k]].mean(axis=1) + rng.normal(0, 0.4 * cell, (n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    length = np.concatenate([rng.uniform(0, 0.45 * cell, n - 10000), rng.uniform(0.5 * cell, 3 * cell, 10000)])
+    starts = np.concatenate([p, v[f[k[:2000], 0]], rng.uniform(lo - 5, hi + 5, (3000, 3))]).astype(np.float32)
+    ends = np.concatenate([p + d * length[:, None], v[f[k[:2000], 0]] + d[:2000] * 0.05,
+                           rng.uniform(lo - 5, hi + 5, (3000, 3))]).astype(np.float32)
+    ends[:3000, 1:] = starts[:3000, 1:]                            # parallel to the x axis
+    got = mesh.segments_blocked(starts, ends, runtime)
+    want = bvh.segment_hits(starts, ends, n_threads=8)[0].astype(bool)
+    assert np.array_equal(got, want), np.flatnonzero(got != want)[:10]
+    assert 0.05 < want.mean() < 0.6
 
 
 def test_contains_matches_oracle(runtime):

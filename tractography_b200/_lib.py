@@ -39,6 +39,7 @@ EXPORTS = (
     "tg_bvh_build_host",
     "tg_mesh_info",
     "tg_mesh_segment_hits",
+    "tg_mesh_segments_blocked",
     "tg_tractogram",
     "tg_tractogram_host",
     "tg_tractogram_noalloc",
@@ -139,6 +140,7 @@ def load() -> ctypes.CDLL:
                               ctypes.c_int),
         "tg_mesh_info": ([P, ctypes.POINTER(U32), ctypes.POINTER(U32), P, ctypes.POINTER(U64)], ctypes.c_int),
         "tg_mesh_segment_hits": ([P, P, P, U32, P, P, P, P], ctypes.c_int),
+        "tg_mesh_segments_blocked": ([P, P, P, U32, P, P], ctypes.c_int),
         "tg_tractogram": ([AP, P, P, P, U32, F, U32, P, P, P], ctypes.c_int),
         "tg_tractogram_host": ([AP, P, P, P, U32, F, U32, P, P, P], ctypes.c_int),
         "tg_tractogram_noalloc": ([AP, P, P, P, U32, U32, P, F, U32, P, P, P], ctypes.c_int),

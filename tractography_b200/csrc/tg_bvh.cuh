@@ -24,7 +24,11 @@
  *     an axis-aligned box of empty cells that is separated from every leaf
  *     box along some axis by more than the rounding of the slab test, so
  *     every leaf slab test fails and the walk would find nothing: the walk is
- *     skipped.  The result is the walk's result in every case.
+ *     skipped.  Near the surface each cell also lists the leaves whose grown
+ *     box meets its half-cell neighbourhood; a short segment starting in the
+ *     cell tests those leaves (independent loads) instead of walking ~2 x
+ *     depth dependent nodes.  The result is the walk's result in every case
+ *     (mesh_segment_blocked gives the argument).
  *
  * Layout (built on the host, tg_mesh.cu):
  *   nodes  2 float4 per node: (min.xyz, skip as uint bits), (max.xyz, leaf
@@ -46,10 +50,14 @@ namespace tg {
 constexpr int kDomainImage = 0;
 constexpr int kDomainMesh = 1;
 
+// Cell word: distance (low 8 bits) | leaf list offset in 16-byte units.
+constexpr uint32_t kNoLeafList = 0xFFFFFFu;
+
 struct MeshDev {
     const float4* nodes;
     const float4* tris;
-    const uint8_t* dist;
+    const uint32_t* cells;   // per grid cell: distance | leaf list offset << 8
+    const uint4* lists;      // leaf lists: count, then leaf node indices
     uint32_t n_nodes;
     float gx, gy, gz;        // grid cells per axis
     float ox, oy, oz;        // grid origin
@@ -212,23 +220,71 @@ __device__ __forceinline__ bool mesh_contains(const MeshDev& m, float x, float y
     return odd >= 2;
 }
 
+// Any hit among the leaves of one cell's list (count, then leaf node
+// indices), with max_t = 1 as in the walk's any-hit mode.  The boxes of four
+// leaves are fetched before they are tested.
+__device__ __forceinline__ bool mesh_leaves_hit(const MeshDev& m, const Segment& g, const uint4* list)
+{
+    const uint32_t* ids = reinterpret_cast<const uint32_t*>(list);
+    const uint32_t count = __ldg(ids);
+#pragma unroll 1
+    for (uint32_t k = 1; k <= count; k += 4) {
+        float4 lo[4], hi[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            // ids past the count are the list's zero padding (node 0, not tested)
+            const uint32_t leaf = __ldg(ids + k + q);
+            lo[q] = __ldg(m.nodes + 2 * (size_t)leaf);
+            hi[q] = __ldg(m.nodes + 2 * (size_t)leaf + 1);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (k + (uint32_t)q > count || !box_hit(g, lo[q], hi[q], 1.0f)) continue;
+            const int code = __float_as_int(hi[q].w);
+            const uint32_t first = (uint32_t)code >> 3;
+            const uint32_t n = (uint32_t)code & 7u;
+            for (uint32_t j = 0; j < n; ++j) {
+                float tt, uu, vv;
+                if (triangle_hit(g, m.tris + 3 * (size_t)(first + j), 1.0f, tt, uu, vv)) return true;
+            }
+        }
+    }
+    return false;
+}
+
 // True when the segment from the last point to the current one hits the
-// surface (the found flag of bvh.cl:83-131), with the distance-grid skip.
+// surface (the found flag of bvh.cl:83-131).  Three routes, one result:
+//   - both ends in cells nearer each other than the start cell's distance:
+//     no leaf box test can pass, nothing is hit;
+//   - both ends inside the start cell's half-cell neighbourhood (with a
+//     0.01-cell allowance for the rounding of the cell coordinates): the
+//     cell's leaf list holds every leaf whose box test can pass.  Rounding
+//     is monotonic, so an ancestor's slab interval contains its leaf's and
+//     an ancestor passes whenever one of its leaves does; the walk therefore
+//     reaches a leaf exactly when the leaf's own box test passes, and the
+//     any-hit over the list equals the walk's;
+//   - otherwise the any-hit walk from the root.
 __device__ __forceinline__ bool mesh_segment_blocked(const MeshDev& m, float sx, float sy, float sz, float ex,
                                                      float ey, float ez)
 {
-    const float ax = floorf((sx - m.ox) * m.inv_cell), ay = floorf((sy - m.oy) * m.inv_cell),
-                az = floorf((sz - m.oz) * m.inv_cell);
-    const float bx = floorf((ex - m.ox) * m.inv_cell), by = floorf((ey - m.oy) * m.inv_cell),
-                bz = floorf((ez - m.oz) * m.inv_cell);
+    const float usx = (sx - m.ox) * m.inv_cell, usy = (sy - m.oy) * m.inv_cell, usz = (sz - m.oz) * m.inv_cell;
+    const float uex = (ex - m.ox) * m.inv_cell, uey = (ey - m.oy) * m.inv_cell, uez = (ez - m.oz) * m.inv_cell;
+    const float ax = floorf(usx), ay = floorf(usy), az = floorf(usz);
+    const float bx = floorf(uex), by = floorf(uey), bz = floorf(uez);
+    const Segment g = make_segment(sx, sy, sz, ex, ey, ez);
     if (ax >= 0.0f && ax < m.gx && ay >= 0.0f && ay < m.gy && az >= 0.0f && az < m.gz && bx >= 0.0f &&
         bx < m.gx && by >= 0.0f && by < m.gy && bz >= 0.0f && bz < m.gz) {
         const size_t cell = ((size_t)ax * (size_t)m.gy + (size_t)ay) * (size_t)m.gz + (size_t)az;
-        const float reach = (float)__ldg(m.dist + cell);
+        const uint32_t word = __ldg(m.cells + cell);
+        const float reach = (float)(word & 255u);
         const float cheb = fmaxf(fmaxf(fabsf(bx - ax), fabsf(by - ay)), fabsf(bz - az));
         if (cheb < reach) return false;
+        const uint32_t list = word >> 8;
+        const float lo = -0.49f, hi = 1.49f;
+        if (list != kNoLeafList && uex - ax >= lo && uex - ax <= hi && uey - ay >= lo && uey - ay <= hi &&
+            uez - az >= lo && uez - az <= hi)
+            return mesh_leaves_hit(m, g, m.lists + list);
     }
-    const Segment g = make_segment(sx, sy, sz, ex, ey, ez);
     float t, u, v;
     uint32_t tri;
     return mesh_walk<1>(m, g, t, tri, u, v) != 0u;

@@ -311,7 +311,8 @@ int tg_domain_destroy(tg_domain* domain)
     if (domain->d.mask) cudaFree(domain->d.mask);
     if (domain->d.nodes) cudaFree(domain->d.nodes);
     if (domain->d.tris) cudaFree(domain->d.tris);
-    if (domain->d.dist) cudaFree(domain->d.dist);
+    if (domain->d.cells) cudaFree(domain->d.cells);
+    if (domain->d.lists) cudaFree(domain->d.lists);
     delete domain;
     return TG_OK;
 }
@@ -384,6 +385,17 @@ int tg_mesh_segment_hits(const tg_domain* domain, const float* starts, const flo
     TG_TRY(launch_mesh_segment_hits(domain->d.mesh, reinterpret_cast<const float4*>(starts),
                                     reinterpret_cast<const float4*>(ends), n, found, triangle,
                                     reinterpret_cast<float4*>(hit), as_stream(stream)));
+    return TG_OK;
+}
+
+int tg_mesh_segments_blocked(const tg_domain* domain, const float* starts, const float* ends, uint32_t n,
+                             uint8_t* blocked, void* stream)
+{
+    if (domain == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "domain is null");
+    if (domain->d.kind != kDomainMesh) return fail(TG_ERR_INVALID_ARGUMENT, "not a mesh domain");
+    if (n == 0) return TG_OK;
+    TG_TRY(launch_mesh_segments_blocked(domain->d.mesh, reinterpret_cast<const float4*>(starts),
+                                        reinterpret_cast<const float4*>(ends), n, blocked, as_stream(stream)));
     return TG_OK;
 }
 

@@ -46,7 +46,8 @@ struct DomainDev {
     // mesh
     float4* nodes = nullptr;
     float4* tris = nullptr;
-    uint8_t* dist = nullptr;
+    uint32_t* cells = nullptr;    // distance | leaf list offset << 8
+    uint32_t* lists = nullptr;
     uint32_t n_triangles = 0;
     MeshDev mesh{};
 };
@@ -214,6 +215,8 @@ struct BoundaryBvhHost {
 int build_boundary_bvh(const double* vertices, uint32_t n_vertices, const uint32_t* faces, uint32_t n_faces,
                        BoundaryBvhHost* out, std::string* error);
 cudaError_t upload_mesh(const BoundaryBvhHost& b, DomainDev* d, cudaStream_t stream);
+cudaError_t launch_mesh_segments_blocked(const MeshDev& m, const float4* starts, const float4* ends, uint32_t n,
+                                         uint8_t* blocked, cudaStream_t stream);
 cudaError_t launch_mesh_segment_hits(const MeshDev& m, const float4* starts, const float4* ends, uint32_t n,
                                      uint8_t* found, uint32_t* triangle, float4* hit, cudaStream_t stream);
 cudaError_t launch_mesh_contains(const MeshDev& m, const float4* points, uint32_t n, uint8_t* out,

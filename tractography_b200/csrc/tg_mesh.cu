@@ -175,8 +175,18 @@ namespace {
 // Distance grid over the root bounds: Chebyshev distance in cells to the
 // nearest cell touched by a leaf box grown by a margin well above the
 // rounding of the cell computation and of the slab test, capped at 255.
+// Beside it, per cell A, the leaves whose grown box meets A's half-cell
+// neighbourhood [A - 0.5, A + 1.5) (cell units, per axis): a segment inside
+// that neighbourhood can pass the box test of no other leaf.  Cell word =
+// distance | (list offset in 16-byte units << 8); a list is its leaf count
+// followed by the leaf node indices (preorder) and zero padding up to
+// 4 * (ceil(count / 4) + 1) words, all that the device's reads of four ids
+// at a time reach; offset 0 is the empty list.  When the offsets would not
+// fit in 24 bits every cell holds kNoLeafList and segments take the walk.
 struct DistanceGrid {
     std::vector<uint8_t> d;
+    std::vector<uint32_t> words;
+    std::vector<uint32_t> lists;
     uint32_t g[3];
     float origin[3];
     float inv_cell;
@@ -251,6 +261,61 @@ DistanceGrid distance_grid(const BoundaryBvhHost& b)
     };
     pass(+1);
     pass(-1);
+
+    // leaf lists: start cells A with A - 0.5 <= hi and A + 1.5 >= lo (grown box, cell units)
+    std::vector<uint32_t> count(gx * gy * gz, 0u);
+    auto start_range = [&](uint32_t i, long a0[3], long a1[3]) {
+        for (int a = 0; a < 3; ++a) {
+            const double l = ((double)b.bounds_min[4 * (size_t)i + a] - margin - (double)G.origin[a]) *
+                             (double)G.inv_cell;
+            const double h = ((double)b.bounds_max[4 * (size_t)i + a] + margin - (double)G.origin[a]) *
+                             (double)G.inv_cell;
+            a0[a] = (long)std::max(0.0, std::ceil(l - 1.5));
+            a1[a] = (long)std::min((double)(G.g[a] - 1), std::floor(h + 0.5));
+            if (a0[a] > a1[a]) return false;
+        }
+        return true;
+    };
+    for (uint32_t i = 0; i < b.n_nodes; ++i) {
+        if (b.nodes[4 * (size_t)i + 3] <= 0) continue;
+        long a0[3], a1[3];
+        if (!start_range(i, a0, a1)) continue;
+        for (long x = a0[0]; x <= a1[0]; ++x)
+            for (long y = a0[1]; y <= a1[1]; ++y)
+                for (long z = a0[2]; z <= a1[2]; ++z) count[((size_t)x * gy + y) * gz + z] += 1u;
+    }
+    std::vector<uint32_t> offset(count.size(), 0u);
+    size_t total = 1;                                        // unit 0: the empty list
+    for (size_t k = 0; k < count.size(); ++k)
+        if (count[k] > 0) {
+            offset[k] = (uint32_t)std::min<size_t>(total, 0xFFFFFFFFu);
+            // count word + ids in 16-byte units, plus the padding that the
+            // device's reads of four ids at a time reach: ceil(count/4) + 1
+            total += (count[k] + 3u) / 4u + 1u;
+        }
+    G.words.assign(count.size(), 0u);
+    if (total <= (size_t)kNoLeafList) {
+        G.lists.assign(4 * (total + 1), 0u);
+        std::vector<uint32_t> fill(count.size(), 0u);
+        for (uint32_t i = 0; i < b.n_nodes; ++i) {
+            if (b.nodes[4 * (size_t)i + 3] <= 0) continue;
+            long a0[3], a1[3];
+            if (!start_range(i, a0, a1)) continue;
+            for (long x = a0[0]; x <= a1[0]; ++x)
+                for (long y = a0[1]; y <= a1[1]; ++y)
+                    for (long z = a0[2]; z <= a1[2]; ++z) {
+                        const size_t k = ((size_t)x * gy + y) * gz + z;
+                        G.lists[4 * (size_t)offset[k] + 1 + fill[k]++] = i;
+                    }
+        }
+        for (size_t k = 0; k < count.size(); ++k) {
+            if (count[k] > 0) G.lists[4 * (size_t)offset[k]] = count[k];
+            G.words[k] = (uint32_t)G.d[k] | (offset[k] << 8);
+        }
+    } else {
+        G.lists.assign(4, 0u);
+        for (size_t k = 0; k < count.size(); ++k) G.words[k] = (uint32_t)G.d[k] | ((uint32_t)kNoLeafList << 8);
+    }
     return G;
 }
 
@@ -294,21 +359,29 @@ cudaError_t upload_mesh(const BoundaryBvhHost& b, DomainDev* d, cudaStream_t str
     const DistanceGrid G = distance_grid(b);
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&d->nodes), nodes.size() * sizeof(float4));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->tris), tris.size() * sizeof(float4));
-    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->dist), G.d.size());
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->cells), G.words.size() * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->lists), G.lists.size() * sizeof(uint32_t));
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d->nodes, nodes.data(), nodes.size() * sizeof(float4), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d->tris, tris.data(), tris.size() * sizeof(float4), cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d->dist, G.d.data(), G.d.size(), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d->cells, G.words.data(), G.words.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                            stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d->lists, G.lists.data(), G.lists.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                            stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return e;
     d->kind = kDomainMesh;
     d->n_triangles = T;
-    d->bytes = nodes.size() * sizeof(float4) + tris.size() * sizeof(float4) + G.d.size();
+    d->bytes = nodes.size() * sizeof(float4) + tris.size() * sizeof(float4) +
+               (G.words.size() + G.lists.size()) * sizeof(uint32_t);
     MeshDev& m = d->mesh;
     m.nodes = d->nodes;
     m.tris = d->tris;
-    m.dist = d->dist;
+    m.cells = d->cells;
+    m.lists = reinterpret_cast<const uint4*>(d->lists);
     m.n_nodes = N;
     m.gx = (float)G.g[0];
     m.gy = (float)G.g[1];
@@ -350,6 +423,24 @@ __global__ void __launch_bounds__(128) mesh_contains_kernel(MeshDev m, const flo
     if (i >= n) return;
     const float4 p = points[i];
     out[i] = mesh_contains(m, p.x, p.y, p.z) ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(128) mesh_segments_blocked_kernel(MeshDev m, const float4* __restrict__ starts,
+                                                                    const float4* __restrict__ ends, uint32_t n,
+                                                                    uint8_t* __restrict__ blocked)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 s = starts[i], e = ends[i];
+    blocked[i] = mesh_segment_blocked(m, s.x, s.y, s.z, e.x, e.y, e.z) ? 1 : 0;
+}
+
+cudaError_t launch_mesh_segments_blocked(const MeshDev& m, const float4* starts, const float4* ends, uint32_t n,
+                                         uint8_t* blocked, cudaStream_t stream)
+{
+    if (n == 0) return cudaSuccess;
+    mesh_segments_blocked_kernel<<<(n + 127) / 128, 128, 0, stream>>>(m, starts, ends, n, blocked);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_mesh_segment_hits(const MeshDev& m, const float4* starts, const float4* ends, uint32_t n,

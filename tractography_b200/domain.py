@@ -294,6 +294,30 @@ class Mesh(BaseDomain):
             return (found.cpu().numpy().astype(bool), tri.cpu().numpy().view(np.uint32),
                     hit.cpu().numpy())
 
+    def segments_blocked(self, starts, ends, runtime=None) -> np.ndarray:
+        """Whether each segment hits the surface, computed as the tracking
+        kernels' domain test computes it (the found flag of
+        bvh_segment_hit, utils/bvh.cl:83-131)."""
+        from .runtime import default_runtime
+
+        import torch
+
+        runtime = runtime or default_runtime()
+        n = len(starts)
+        if n == 0:
+            return np.zeros(0, bool)
+        s4 = np.zeros((n, 4), np.float32)
+        e4 = np.zeros((n, 4), np.float32)
+        s4[:, :3], e4[:, :3] = np.asarray(starts)[:, :3], np.asarray(ends)[:, :3]
+        with runtime.device_scope():
+            handle = self.device(runtime)
+            ds, de = runtime.to_device(s4), runtime.to_device(e4)
+            out = runtime.empty((n,), torch.uint8)
+            _lib.check(runtime.lib.tg_mesh_segments_blocked(
+                handle, ctypes.c_void_p(ds.data_ptr()), ctypes.c_void_p(de.data_ptr()), n,
+                ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(runtime.stream_handle)))
+            return out.cpu().numpy().astype(bool)
+
 
 def contains(domain: BaseDomain, points, runtime=None) -> np.ndarray:
     """GPU membership test (domain.py:433-491)."""
