@@ -82,6 +82,8 @@ def parse_args():
                         "serving under Poisson load")
     p.add_argument("--rates", default="5,20,50,100,200", help="serving: arrival rates (requests/s)")
     p.add_argument("--duration", type=float, default=6.0, help="serving: seconds of arrivals per rate")
+    p.add_argument("--epoch-steps", type=int, default=65536, help="serving: step cap of an epoch")
+    p.add_argument("--epoch-ms", type=float, default=6.0, help="serving: device-clock budget of an epoch (ms)")
     p.add_argument("--jobs", type=int, default=64, help="jobs of the mixed workload")
     return p.parse_args()
 
@@ -926,8 +928,8 @@ def run_serve(args):
             n_req = max(5, int(rate * args.duration))
             arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
             offered = 0
-            server = Server(runtime, hbm_budget_bytes=150e9 - resident, pool_points=256 << 20, epoch_steps=1024,
-                            max_requests=128)
+            server = Server(runtime, hbm_budget_bytes=150e9 - resident, pool_points=256 << 20,
+                            epoch_steps=args.epoch_steps, epoch_seconds=args.epoch_ms * 1e-3, max_requests=128)
             latency, seeds_done = [], 0
             t0 = time.perf_counter()
             submitted = 0
@@ -956,6 +958,7 @@ def run_serve(args):
             sweep.append({"rate_per_s": rate, "requests": n_req, "p50_s": float(np.percentile(lat, 50)),
                           "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
                           "steps": st.steps, "epochs": st.epochs, "busy_s": st.busy_seconds, "wall_s": wall,
+                          "kernel_s": st.kernel_seconds, "harvest_s": st.harvest_seconds,
                           "steps_per_s": st.steps / max(1e-9, st.busy_seconds),
                           "streamlines_per_s": seeds_done / max(1e-9, st.busy_seconds),
                           "offered_seeds_per_s": float(offered / arrivals[-1])})
@@ -965,7 +968,8 @@ def run_serve(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator; no dataset)", "workload": "serve",
             "config": {"workload": SERVE_WORKLOAD, "rates_per_s": rates, "arrival_seconds": args.duration,
-                       "epoch_steps": 1024, "latency": "submission to completion on the device (all streamlines "
+                       "epoch_steps": args.epoch_steps, "epoch_ms": args.epoch_ms,
+                       "latency": "submission to completion on the device (all streamlines "
                                                        "harvested into the request's result buffer)"},
             "sweep": sweep, "clocks": sampler.summary()}
     print(json.dumps(line), flush=True)

@@ -2,7 +2,8 @@
 
 Requests of several code paths (SH lmax 4/8, tensor; Transport and
 Diffusion; image and mesh domains) arrive in waves while others run.  Short
-epochs force streamlines to be carried across many epochs, and a small
+epochs (by step count or by a device-clock deadline) force streamlines to be
+carried across many epochs, and a small
 point pool forces re-queued streamlines; neither may change a result: each
 request must equal, bit for bit, the same job tracked alone by the packed
 tracker (tg_tracker_run), and a few equal the CPU oracle directly.
@@ -61,12 +62,13 @@ def run_alone(job, runtime):
                                     philox_key=job.philox_key)
 
 
-@pytest.mark.parametrize("epoch_steps,pool_points", [(1024, 0), (7, 0), (64, 6000)])
-def test_requests_equal_alone_in_the_mix(runtime, epoch_steps, pool_points):
+@pytest.mark.parametrize("epoch_steps,pool_points,epoch_seconds",
+                         [(1024, 0, 0.0), (7, 0, 0.0), (64, 6000, 0.0), (1 << 16, 0, 2e-5)])
+def test_requests_equal_alone_in_the_mix(runtime, epoch_steps, pool_points, epoch_seconds):
     jobs = make_jobs()
     alone = [run_alone(j, runtime) for j in jobs]
     server = Server(runtime, hbm_budget_bytes=8e9, pool_points=pool_points, epoch_steps=epoch_steps,
-                    max_requests=5)
+                    max_requests=5, epoch_seconds=epoch_seconds)
     ids = {}
     results = {}
     waves = [jobs[:4], jobs[4:9], jobs[9:]]
@@ -94,6 +96,7 @@ def test_requests_equal_alone_in_the_mix(runtime, epoch_steps, pool_points):
         assert len(points) == int(lengths.sum()) and seconds > 0
     # short epochs carry streamlines across many epochs
     assert stats.epochs >= (2 if epoch_steps >= 1024 else 20)
+    assert stats.kernel_seconds > 0.0 and stats.harvest_seconds >= 0.0
 
 
 def test_server_matches_oracle(runtime):

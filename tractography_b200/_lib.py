@@ -58,6 +58,8 @@ EXPORTS = (
     "tg_server_result_size",
     "tg_server_take",
     "tg_server_stats",
+    "tg_server_set_epoch_time",
+    "tg_server_timing",
     "tg_seeds_from_fod",
     "tg_domain_contains",
     "tg_field_evaluate",
@@ -161,6 +163,8 @@ def load() -> ctypes.CDLL:
         "tg_server_result_size": ([P, U64, ctypes.POINTER(U32), ctypes.POINTER(U64), ctypes.POINTER(ctypes.c_double)],
                                   ctypes.c_int),
         "tg_server_take": ([P, U64, P, P, P], ctypes.c_int),
+        "tg_server_set_epoch_time": ([P, ctypes.c_double], ctypes.c_int),
+        "tg_server_timing": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "tg_server_stats": ([P, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(ctypes.c_double),
                              ctypes.POINTER(U64)], ctypes.c_int),
         "tg_seeds_from_fod": ([I32, U32, P, P, U32, P, P, U32, P, P], ctypes.c_int),

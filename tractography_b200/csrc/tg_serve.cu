@@ -12,9 +12,12 @@
  *   - an epoch launches one persistent kernel per code path with work, on
  *     concurrent streams.  Lanes first resume the streamlines carried over
  *     from the previous epoch, then take new seeds from the queue; every lane
- *     executes at most `epoch_steps` loop iterations, after which a live
- *     streamline is saved (position, orientation, RNG state, output cursor)
- *     and resumed in the next epoch.  Requests that arrive while others run
+ *     executes at most `epoch_steps` loop iterations and, when an epoch time
+ *     is set, stops at the epoch's deadline on the device clock (so code
+ *     paths with costlier steps, e.g. closed-surface domains, end with the
+ *     rest instead of holding the GPU), after which a live streamline is
+ *     saved (position, orientation, RNG state, output cursor) and resumed in
+ *     the next epoch.  Requests that arrive while others run
  *     enter at the next epoch, so a small request never waits for the tail
  *     of a large one, and lanes freed by finished streamlines are refilled
  *     from any request of the same code path;
@@ -112,10 +115,24 @@ struct ServeParams {
     uint32_t n_new;
     unsigned long long* counter;
     uint32_t step_budget;
+    const unsigned long long* deadline;   // epoch end on the device clock (ns); null: steps only
     unsigned long long* steps_done;
     Finished* finished;          // streamlines that finished this epoch
     unsigned int* n_finished;
 };
+
+__device__ __forceinline__ unsigned long long device_clock_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// The epoch's deadline: now + budget on the device clock.
+__global__ void epoch_deadline_kernel(unsigned long long* deadline, unsigned long long budget_ns)
+{
+    *deadline = device_clock_ns() + budget_ns;
+}
 
 __device__ __forceinline__ uint32_t seg_upper_bound(const uint32_t* a, uint32_t n, uint32_t v)
 {
@@ -170,6 +187,7 @@ __global__ void __launch_bounds__(128, 5) serve_kernel(const ServeParams sp)
     uint32_t slot = 0, item = 0, fill = 0;
     int32_t chunk = -1;
     uint32_t budget = sp.step_budget;
+    const unsigned long long deadline = sp.deadline != nullptr ? *sp.deadline : ~0ull;
     unsigned long long steps_total = 0;
 
     // Reserve the streamline's worst-case chunks, take its first chunk and
@@ -224,6 +242,15 @@ __global__ void __launch_bounds__(128, 5) serve_kernel(const ServeParams sp)
     while (true) {
         const unsigned active = __ballot_sync(0xffffffffu, live);
         if (active == 0u) break;
+        // the epoch ends after step_budget iterations or at the deadline,
+        // read by lane 0 every 8 iterations (the whole warp stops together);
+        // every warp runs at least 8 iterations, so every epoch makes progress
+        const uint32_t used = sp.step_budget - budget;
+        if (budget != 0u && used != 0u && (used & 7u) == 0u && deadline != ~0ull) {
+            unsigned long long now = 0;
+            if ((threadIdx.x & 31u) == 0u) now = device_clock_ns();
+            if (__shfl_sync(0xffffffffu, now, 0) > deadline) budget = 0u;
+        }
         if (budget == 0u) {
             if (live) lane_save(sp.carry_out + atomicAdd(sp.carry_out_count, 1u), s, item, chunk, fill, slot);
             break;
@@ -352,6 +379,18 @@ __global__ void __launch_bounds__(256) harvest_kernel(const ServeJob* __restrict
             J.result_offset[f.item] = off;
         }
         off = __shfl_sync(0xffffffffu, off, 0);
+        // lane q holds the q-th chunk of the current group of up to 32;
+        // each group goes back to the free list with one atomic
+        int32_t held = -1;
+        uint32_t n_held = 0, n_freed = 0;
+        auto give_back = [&]() {
+            unsigned int at = 0;
+            if (lane == 0) at = atomicAdd(alloc, n_held);
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (lane < n_held) free_list[at + lane] = held;
+            n_freed += n_held;
+            n_held = 0;
+        };
         for (uint32_t base = 0; base < len && chunk >= 0; base += kChunkPoints) {
             const uint32_t j = base + lane;
             if (j < len) {
@@ -361,14 +400,13 @@ __global__ void __launch_bounds__(256) harvest_kernel(const ServeJob* __restrict
                 dst[1] = src[1];
                 dst[2] = src[2];
             }
-            const int32_t next = chunk_next[chunk];
-            __syncwarp();
-            if (lane == 0) {
-                free_list[atomicAdd(alloc, 1u)] = chunk;
-                atomicAdd(committed, (unsigned long long)-1ll);
-            }
-            chunk = next;
+            if (lane == n_held) held = chunk;
+            n_held += 1;
+            chunk = chunk_next[chunk];
+            if (n_held == 32u) give_back();
         }
+        if (n_held > 0u) give_back();
+        if (lane == 0 && n_freed > 0u) atomicAdd(committed, (unsigned long long)(-(long long)n_freed));
     }
 }
 
@@ -474,6 +512,15 @@ struct tg_server {
     uint64_t steps_total = 0;
     uint64_t epochs = 0;
     double busy_s = 0.0;
+    // device-clock epoch budget (0: epoch_steps only) and device timing
+    uint64_t epoch_ns = 0;
+    unsigned long long* d_deadline = nullptr;
+    cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr, ev_t2 = nullptr;
+    double kernel_s = 0.0, harvest_s = 0.0;
+    // request buffers come from the server's own pool, which keeps freed
+    // memory (up to the budget) for the next requests instead of returning
+    // it to the driver at every synchronisation
+    cudaMemPool_t mempool = nullptr;
 };
 
 namespace {
@@ -526,12 +573,12 @@ int admit(tg_server* S)
         if (slot < 0 || S->fixed + S->reserved + r->reserve > S->budget) return TG_OK;
         const uint32_t n = r->job.n_seeds;
         r->result_cap = std::max<uint64_t>(1024, (uint64_t)n * std::min<uint64_t>(r->job.n_steps, S->points_estimate));
-        TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&r->d_seeds), (size_t)n * 32, S->stream));
-        TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&r->d_rng), (size_t)r->n_batches * 4, S->stream));
-        TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&r->d_lengths), (size_t)n * 4, S->stream));
-        TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&r->d_first), (size_t)n * 4, S->stream));
-        TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&r->d_offset), (size_t)n * 8, S->stream));
-        TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&r->d_result), r->result_cap * 12, S->stream));
+        TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_seeds), (size_t)n * 32, S->mempool, S->stream));
+        TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_rng), (size_t)r->n_batches * 4, S->mempool, S->stream));
+        TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_lengths), (size_t)n * 4, S->mempool, S->stream));
+        TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_first), (size_t)n * 4, S->mempool, S->stream));
+        TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_offset), (size_t)n * 8, S->mempool, S->stream));
+        TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_result), r->result_cap * 12, S->mempool, S->stream));
         // pageable copies are staged before cudaMemcpyAsync returns
         TG_STRY(cudaMemcpyAsync(r->d_seeds, r->host_seeds, (size_t)n * 32, cudaMemcpyHostToDevice, S->stream));
         TG_STRY(cudaMemcpyAsync(r->d_rng, r->host_rng, (size_t)r->n_batches * 4, cudaMemcpyHostToDevice, S->stream));
@@ -633,7 +680,7 @@ int requeue_overflow(tg_server* S, int slot)
         if (len[i] & kOverflowBit) ids.push_back(i);
     if (!ids.empty()) {
         uint32_t* d_ids = nullptr;
-        TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&d_ids), ids.size() * 4, S->stream));
+        TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d_ids), ids.size() * 4, S->mempool, S->stream));
         TG_STRY(cudaMemcpyAsync(d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, S->stream));
         release_kernel<<<((uint32_t)ids.size() + 127) / 128, 128, 0, S->stream>>>(
             S->P.chunk_next, r->d_first, r->d_lengths, d_ids, (uint32_t)ids.size(), S->P.free_list, S->P.alloc,
@@ -658,7 +705,7 @@ int grow_result(tg_server* S, int slot, uint64_t need)
     ServeRequest* r = S->slots[slot];
     uint64_t cap = std::max<uint64_t>(need, r->result_cap + r->result_cap / 2);
     float* fresh = nullptr;
-    TG_STRY(cudaMallocAsync(reinterpret_cast<void**>(&fresh), cap * 12, S->stream));
+    TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&fresh), cap * 12, S->mempool, S->stream));
     if (r->harvested > 0)
         TG_STRY(cudaMemcpyAsync(fresh, r->d_result, r->harvested * 12, cudaMemcpyDeviceToDevice, S->stream));
     TG_STRY(cudaFreeAsync(r->d_result, S->stream));
@@ -695,6 +742,22 @@ int tg_server_create(uint64_t hbm_budget_bytes, uint64_t pool_points, uint32_t e
     S->n_chunks = (uint32_t)chunks;
     cudaError_t e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreate(&S->ev_t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&S->ev_t1);
+    if (e == cudaSuccess) e = cudaEventCreate(&S->ev_t2);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->d_deadline), sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        e = cudaMemPoolCreate(&S->mempool, &props);
+        if (e == cudaSuccess) {
+            uint64_t keep = hbm_budget_bytes;
+            e = cudaMemPoolSetAttribute(S->mempool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->d_jobs), max_requests * sizeof(ServeJob));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->d_counts), 2 * max_requests * sizeof(unsigned int));
     if (e == cudaSuccess)
@@ -755,9 +818,12 @@ int tg_server_destroy(tg_server* S)
     }
     void* bufs[] = {S->d_jobs, S->d_counts, S->d_slot_points, S->P.pool, S->P.chunk_next, S->P.free_list,
                     S->P.alloc, S->P.committed, S->d_carry_count, S->d_counter, S->d_steps, S->d_segs, S->d_finished,
-                    S->d_n_finished};
+                    S->d_n_finished, S->d_deadline};
     for (void* b : bufs) cudaFree(b);
-    if (S->ev_fork) cudaEventDestroy(S->ev_fork);
+    if (S->mempool) cudaMemPoolDestroy(S->mempool);
+    cudaEvent_t evs[] = {S->ev_fork, S->ev_t0, S->ev_t1, S->ev_t2};
+    for (cudaEvent_t ev : evs)
+        if (ev) cudaEventDestroy(ev);
     if (S->stream) cudaStreamDestroy(S->stream);
     delete S;
     return TG_OK;
@@ -896,6 +962,11 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
         TG_STRY(cudaMemsetAsync(S->d_counter, 0, kServeKinds * sizeof(unsigned long long), S->stream));
         TG_STRY(cudaMemsetAsync(S->d_carry_count, 0, kServeKinds * sizeof(unsigned int), S->stream));
         TG_STRY(cudaMemsetAsync(S->d_n_finished, 0, sizeof(unsigned int), S->stream));
+        TG_STRY(cudaEventRecord(S->ev_t0, S->stream));
+        if (S->epoch_ns > 0) {
+            epoch_deadline_kernel<<<1, 1, 0, S->stream>>>(S->d_deadline, (unsigned long long)S->epoch_ns);
+            TG_STRY(cudaGetLastError());
+        }
         TG_STRY(cudaEventRecord(S->ev_fork, S->stream));
         for (int k = 0; k < kServeKinds; ++k) {
             if (grid[k] == 0) continue;
@@ -914,6 +985,7 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
             sp.n_new = (uint32_t)n_new[k];
             sp.counter = S->d_counter + k;
             sp.step_budget = S->epoch_steps;
+            sp.deadline = S->epoch_ns > 0 ? S->d_deadline : nullptr;
             sp.steps_done = S->d_steps;
             sp.finished = S->d_finished;
             sp.n_finished = S->d_n_finished;
@@ -922,6 +994,7 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
             TG_STRY(cudaEventRecord(S->kdone[k], S->kstream[k]));
             TG_STRY(cudaStreamWaitEvent(S->stream, S->kdone[k], 0));
         }
+        TG_STRY(cudaEventRecord(S->ev_t1, S->stream));
         pool_settle_kernel<<<1, 1, 0, S->stream>>>(S->P.alloc);
         TG_STRY(cudaGetLastError());
         unsigned long long counter[kServeKinds];
@@ -961,6 +1034,7 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
                                                           S->P.committed);
             TG_STRY(cudaGetLastError());
         }
+        TG_STRY(cudaEventRecord(S->ev_t2, S->stream));
         for (uint32_t slot : order) {
             if (slot_points[2 * slot] != 0)
                 TG_STRY(cudaMemsetAsync(S->d_slot_points + 2 * slot, 0, sizeof(unsigned long long), S->stream));
@@ -996,6 +1070,9 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
         }
         TG_STRY(cudaStreamSynchronize(S->stream));
         S->busy_s += now_s() - t0;
+        float k_ms = 0.0f, h_ms = 0.0f;
+        if (cudaEventElapsedTime(&k_ms, S->ev_t0, S->ev_t1) == cudaSuccess) S->kernel_s += 1e-3 * k_ms;
+        if (cudaEventElapsedTime(&h_ms, S->ev_t1, S->ev_t2) == cudaSuccess) S->harvest_s += 1e-3 * h_ms;
         st = admit(S);
         if (st != TG_OK) return st;
     }
@@ -1043,6 +1120,22 @@ int tg_server_take(tg_server* S, uint64_t request_id, uint32_t* lengths, uint64_
     S->reserved -= std::min(S->reserved, res.bytes);
     S->results.erase(it);
     return admit(S);
+}
+
+int tg_server_set_epoch_time(tg_server* S, double seconds)
+{
+    if (S == nullptr) return sfail(TG_ERR_INVALID_ARGUMENT, "server is null");
+    if (!(seconds >= 0.0) || seconds > 60.0) return sfail(TG_ERR_INVALID_ARGUMENT, "epoch time must be 0..60 s");
+    S->epoch_ns = (uint64_t)(seconds * 1e9);
+    return TG_OK;
+}
+
+int tg_server_timing(const tg_server* S, double* kernel_seconds, double* harvest_seconds)
+{
+    if (S == nullptr) return sfail(TG_ERR_INVALID_ARGUMENT, "server is null");
+    if (kernel_seconds) *kernel_seconds = S->kernel_s;
+    if (harvest_seconds) *harvest_seconds = S->harvest_s;
+    return TG_OK;
 }
 
 int tg_server_stats(const tg_server* S, uint64_t* steps, uint64_t* epochs, double* busy_seconds,

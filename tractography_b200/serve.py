@@ -32,8 +32,10 @@ from .streamlines import ArraySequence, Tractogram
 class ServerStats:
     steps: int
     epochs: int
-    busy_seconds: float
+    busy_seconds: float          # host wall time of the epochs
     reserved_bytes: int
+    kernel_seconds: float = 0.0  # device time of the epochs' tracking launches
+    harvest_seconds: float = 0.0 # device time of moving finished streamlines to their results
 
 
 class Server:
@@ -47,10 +49,12 @@ class Server:
         pool_points: capacity of the shared point pool (0: 32M points).
         epoch_steps: loop iterations per lane per epoch.
         max_requests: admitted requests at a time.
+        epoch_seconds: device-clock budget of an epoch (0: epoch_steps
+            alone ends it); every code path stops at the same deadline.
     """
 
     def __init__(self, runtime=None, *, hbm_budget_bytes: float = 150e9, pool_points: int = 0,
-                 epoch_steps: int = 1024, max_requests: int = 256):
+                 epoch_steps: int = 1024, max_requests: int = 256, epoch_seconds: float = 0.0):
         from .runtime import default_runtime
 
         self.runtime = runtime or default_runtime()
@@ -59,6 +63,8 @@ class Server:
         with self.runtime.device_scope():
             _lib.check(self.lib.tg_server_create(int(hbm_budget_bytes), int(pool_points), int(epoch_steps),
                                                  int(max_requests), ctypes.byref(self._handle)))
+            if epoch_seconds:
+                _lib.check(self.lib.tg_server_set_epoch_time(self._handle, float(epoch_seconds)))
         self._jobs = {}
         self._arrays = {}
         self._ids = (ctypes.c_uint64 * 1024)()
@@ -146,7 +152,9 @@ class Server:
         steps, epochs, busy, reserved = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double(), ctypes.c_uint64()
         _lib.check(self.lib.tg_server_stats(self._handle, ctypes.byref(steps), ctypes.byref(epochs),
                                             ctypes.byref(busy), ctypes.byref(reserved)))
-        return ServerStats(steps.value, epochs.value, busy.value, reserved.value)
+        kernel, harvest = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.lib.tg_server_timing(self._handle, ctypes.byref(kernel), ctypes.byref(harvest)))
+        return ServerStats(steps.value, epochs.value, busy.value, reserved.value, kernel.value, harvest.value)
 
     def drain(self) -> dict:
         """Poll until every submitted request finished; returns {id: Tractogram}."""
