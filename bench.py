@@ -85,6 +85,8 @@ def parse_args():
     p.add_argument("--epoch-steps", type=int, default=65536, help="serving: step cap of an epoch")
     p.add_argument("--epoch-ms", type=float, default=6.0, help="serving: device-clock budget of an epoch (ms)")
     p.add_argument("--jobs", type=int, default=64, help="jobs of the mixed workload")
+    p.add_argument("--per-class", action="store_true",
+                   help="mixed: also time each code path's jobs alone (persistent and plain)")
     return p.parse_args()
 
 
@@ -557,8 +559,9 @@ def run_mixed(args):
         total, steps = ctypes.c_uint64(), ctypes.c_uint64()
         kms, waves, launches = ctypes.c_float(), ctypes.c_uint32(), ctypes.c_uint32()
 
-        def persistent():
-            _lib.check(lib.tg_tracker_run_jobs(runtime.tracker(), structs, len(jobs), 0,
+        def persistent(subset=None):
+            table, n = (structs, len(jobs)) if subset is None else subset
+            _lib.check(lib.tg_tracker_run_jobs(runtime.tracker(), table, n, 0,
                                                lengths.ctypes.data_as(ctypes.c_void_p),
                                                offsets.ctypes.data_as(ctypes.c_void_p), ctypes.byref(total),
                                                ctypes.byref(steps), sh))
@@ -570,10 +573,13 @@ def run_mixed(args):
         d_out = torch.empty((max_batch * max_steps * 4,), dtype=torch.float32, device=runtime.device)
         d_len = torch.empty((n_total,), dtype=torch.int32, device=runtime.device)
 
-        def plain():
+        def plain(only=None):
             n_launch = 0
             base = 0
             for k, job in enumerate(jobs):
+                if only is not None and k not in only:
+                    base += job.n_seeds
+                    continue
                 d_h, f_h = tracking._handles(job.algorithm, job.domain, job.field, runtime)
                 for b in range(len(job.batch_rng_seeds)):
                     lo = b * job.batch_size
@@ -606,7 +612,38 @@ def run_mixed(args):
             torch.cuda.synchronize()
             q_ms += ev0.elapsed_time(ev1)
         plain_len = d_len.cpu().numpy().view(np.uint32)
-    work = int(steps.value)
+        work = int(steps.value)
+        persistent_kernel_ms = float(kms.value)
+        persistent_launches = int(launches.value)
+        classes = []
+        if args.per_class:
+            # each code path's jobs alone: the multi-job run restricted to them, and their plain launches
+            groups = {}
+            for k, job in enumerate(jobs):
+                key = (type(job.algorithm.local_model).__name__, job.algorithm.local_model.n_parameters,
+                       type(job.algorithm).__name__)
+                groups.setdefault(key, []).append(k)
+            for key, members in sorted(groups.items()):
+                sub = (_lib.Job * len(members))(*[structs[k] for k in members])
+                persistent((sub, len(members)))
+                torch.cuda.synchronize()
+                ev0.record(runtime.stream)
+                persistent((sub, len(members)))
+                ev1.record(runtime.stream)
+                torch.cuda.synchronize()
+                c_ms, c_kernel, c_steps = ev0.elapsed_time(ev1), float(kms.value), int(steps.value)
+                plain(set(members))
+                torch.cuda.synchronize()
+                ev0.record(runtime.stream)
+                plain(set(members))
+                ev1.record(runtime.stream)
+                torch.cuda.synchronize()
+                q = ev0.elapsed_time(ev1)
+                classes.append({"model": key[0], "coefficients": key[1], "algorithm": key[2], "jobs": len(members),
+                                "seeds": int(sum(jobs[k].n_seeds for k in members)), "steps": c_steps,
+                                "persistent_ms": c_ms, "persistent_kernel_ms": c_kernel, "plain_ms": q,
+                                "persistent_kernel_steps_per_s": c_steps / (c_kernel / 1e3),
+                                "plain_steps_per_s": c_steps / (q / 1e3), "speedup_kernel_vs_plain": q / c_kernel})
     line = {
         "metric": METRIC, "workload": "mixed", "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
@@ -616,7 +653,8 @@ def run_mixed(args):
         "speedup_vs_plain": q_ms / p_ms,
         "ms_per_step": p_ms / args.steps,
         "plain_ms_per_step": q_ms / args.steps,
-        "gpu_launches_per_step": int(launches.value),
+        "gpu_launches_per_step": persistent_launches,
+        "kernel_ms_per_step": persistent_kernel_ms,
         "plain_launches_per_step": n_plain,
         "identical_lengths": bool(np.array_equal(plain_len, lengths)),
         "config": {
@@ -627,6 +665,8 @@ def run_mixed(args):
             "plain": "one tg_tractogram launch per 50000-seed batch, jobs in order, dense output",
         },
     }
+    if classes:
+        line["classes"] = classes
     print(json.dumps(line), flush=True)
 
 
