@@ -66,24 +66,58 @@ __device__ __forceinline__ bool locate(const TrackParams& p, Lane& s, float (&c)
         ay = dot4(p.dgrid.row1, s.px, s.py, s.pz, 1.0f);
         az = dot4(p.dgrid.row2, s.px, s.py, s.pz, 1.0f);
         const float vx = floorf(ax + 0.5f), vy = floorf(ay + 0.5f), vz = floorf(az + 0.5f);
-        if (vx != s.dvx || vy != s.dvy || vz != s.dvz) {
-            if (!(vx >= 0.0f && vx < (float)p.dgrid.nx && vy >= 0.0f && vy < (float)p.dgrid.ny &&
-                  vz >= 0.0f && vz < (float)p.dgrid.nz))
-                return false;
+        float bx = ax, by = ay, bz = az;
+        if (!p.same_grid) {
+            bx = dot4(p.fgrid.row0, s.px, s.py, s.pz, 1.0f);
+            by = dot4(p.fgrid.row1, s.px, s.py, s.pz, 1.0f);
+            bz = dot4(p.fgrid.row2, s.px, s.py, s.pz, 1.0f);
+        }
+        const float fx = rintf(bx), fy = rintf(by), fz = rintf(bz);
+        const bool dchange = vx != s.dvx || vy != s.dvy || vz != s.dvz;
+        const bool fchange = fx != s.fvx || fy != s.fvy || fz != s.fvz;
+        // Every failed test stops the streamline the same way, so both bounds
+        // tests come first and the mask byte and the coefficients are then
+        // fetched together: one memory round trip per voxel change, not two.
+        // (A streamline stopped by its mask leaves c overwritten; nothing
+        // reads c after a stop.)
+        if (dchange && !(vx >= 0.0f && vx < (float)p.dgrid.nx && vy >= 0.0f && vy < (float)p.dgrid.ny &&
+                         vz >= 0.0f && vz < (float)p.dgrid.nz))
+            return false;
+        if (fchange && !(fx >= 0.0f && fx < (float)p.fgrid.nx && fy >= 0.0f && fy < (float)p.fgrid.ny &&
+                         fz >= 0.0f && fz < (float)p.fgrid.nz))
+            return false;
+        uint8_t inside = 1;
+        if (dchange) {
             const int64_t k = ((int64_t)(int32_t)vx * p.dgrid.ny + (int32_t)vy) * p.dgrid.nz + (int32_t)vz;
-            if (__ldg(p.mask + k) == 0) return false;
+            inside = __ldg(p.mask + k);
+        }
+        if (fchange) {
+            const int64_t fv = ((int64_t)(int32_t)fx * p.fgrid.ny + (int32_t)fy) * p.fgrid.nz + (int32_t)fz;
+            const float4* src = reinterpret_cast<const float4*>(p.field) + fv * (CPAD / 4);
+#pragma unroll
+            for (int k = 0; k < CPAD / 4; ++k) {
+                const float4 v = __ldg(src + k);
+                c[4 * k] = v.x;
+                c[4 * k + 1] = v.y;
+                c[4 * k + 2] = v.z;
+                c[4 * k + 3] = v.w;
+            }
+        }
+        if (inside == 0) return false;
+        if (dchange) {
             s.dvx = vx;
             s.dvy = vy;
             s.dvz = vz;
         }
+        if (fchange) {
+            s.fvx = fx;
+            s.fvy = fy;
+            s.fvz = fz;
+        }
+        return true;
     }
-    float bx = ax, by = ay, bz = az;
-    if (DOM == kDomainImage && !p.same_grid) {
-        bx = dot4(p.fgrid.row0, s.px, s.py, s.pz, 1.0f);
-        by = dot4(p.fgrid.row1, s.px, s.py, s.pz, 1.0f);
-        bz = dot4(p.fgrid.row2, s.px, s.py, s.pz, 1.0f);
-    }
-    const float fx = rintf(bx), fy = rintf(by), fz = rintf(bz);
+    // closed surface: the field gather of the point (ax, ay, az are field-voxel coordinates)
+    const float fx = rintf(ax), fy = rintf(ay), fz = rintf(az);
     if (fx != s.fvx || fy != s.fvy || fz != s.fvz) {
         if (!(fx >= 0.0f && fx < (float)p.fgrid.nx && fy >= 0.0f && fy < (float)p.fgrid.ny &&
               fz >= 0.0f && fz < (float)p.fgrid.nz))
