@@ -40,6 +40,13 @@ struct tg_tracker {
     uint32_t* ids = nullptr;
     uint32_t* done_ids = nullptr;
     size_t cap_seeds = 0;
+    // device offsets of a run whose streamlines all fit the pool
+    uint64_t* masked = nullptr;
+    size_t cap_masked = 0;
+    uint8_t* scan_temp = nullptr;
+    size_t cap_scan_temp = 0;
+    unsigned long long* d_totals = nullptr;
+    size_t cap_totals = 0;
     float4* seeds = nullptr;
     size_t cap_seed_copy = 0;
     uint32_t* batch_seeds = nullptr;
@@ -478,6 +485,9 @@ int tg_tracker_destroy(tg_tracker* t)
     cudaFree(t->offsets);
     cudaFree(t->ids);
     cudaFree(t->done_ids);
+    cudaFree(t->masked);
+    cudaFree(t->scan_temp);
+    cudaFree(t->d_totals);
     cudaFree(t->seeds);
     cudaFree(t->batch_seeds);
     cudaFree(t->points);
@@ -711,6 +721,38 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
             t->launches += 1;
         }
         TG_TRY(cudaEventRecord(t->ev_stop, s));
+        if (first_wave) {
+            // Common case: every streamline fit the pool; offsets by a device
+            // scan (tg_tracker_run_jobs does the same).
+            size_t temp_bytes = 0;
+            TG_TRY(launch_offsets(t->lengths, n_seeds, nullptr, nullptr, nullptr, nullptr, &temp_bytes, s));
+            TG_TRY(ensure(&t->masked, &t->cap_masked, n_seeds));
+            TG_TRY(ensure(&t->scan_temp, &t->cap_scan_temp, temp_bytes));
+            TG_TRY(ensure(&t->d_totals, &t->cap_totals, 2));
+            TG_TRY(launch_offsets(t->lengths, n_seeds, t->masked, t->offsets, t->d_totals, t->scan_temp, &temp_bytes,
+                                  s));
+            unsigned long long totals[2] = {0ull, 0ull};
+            TG_TRY(cudaMemcpyAsync(totals, t->d_totals, sizeof totals, cudaMemcpyDeviceToHost, s));
+            TG_TRY(cudaStreamSynchronize(s));
+            if (totals[1] == 0ull) {
+                float wave_ms = 0.0f;
+                TG_TRY(cudaEventElapsedTime(&wave_ms, t->ev_start, t->ev_stop));
+                t->kernel_ms += wave_ms;
+                t->waves += 1;
+                total = totals[0];
+                st = tracker_points(t, total, s);
+                if (st != TG_OK) return st;
+                TG_TRY(launch_gather(t->pool, t->chunk_next, t->first_chunk, t->lengths, t->offsets, nullptr, n_seeds,
+                                     t->points, s));
+                t->launches += 1;
+                t->total_points = total;
+                TG_TRY(cudaMemcpyAsync(h_lengths, t->lengths, (size_t)n_seeds * sizeof(uint32_t),
+                                       cudaMemcpyDeviceToHost, s));
+                TG_TRY(cudaMemcpyAsync(h_offsets, t->offsets, (size_t)n_seeds * sizeof(uint64_t),
+                                       cudaMemcpyDeviceToHost, s));
+                break;
+            }
+        }
         TG_TRY(cudaMemcpyAsync(t->h_len.data(), t->lengths, (size_t)n_seeds * sizeof(uint32_t),
                                cudaMemcpyDeviceToHost, s));
         TG_TRY(cudaStreamSynchronize(s));
@@ -988,6 +1030,37 @@ int tg_tracker_run_jobs(tg_tracker* t, const tg_job* jobs, uint32_t n_jobs, int 
             launched.push_back(k);
         }
         TG_TRY(cudaEventRecord(t->ev_stop, s));
+        if (first_wave) {
+            // Common case: every streamline fit the pool.  Offsets come from a
+            // device scan of the lengths (streamlines packed in seed order) and
+            // the host reads two totals instead of visiting every seed.
+            size_t temp_bytes = 0;
+            TG_TRY(launch_offsets(t->lengths, (uint32_t)n_total, nullptr, nullptr, nullptr, nullptr, &temp_bytes, s));
+            TG_TRY(ensure(&t->masked, &t->cap_masked, n_total));
+            TG_TRY(ensure(&t->scan_temp, &t->cap_scan_temp, temp_bytes));
+            TG_TRY(ensure(&t->d_totals, &t->cap_totals, 2));
+            TG_TRY(launch_offsets(t->lengths, (uint32_t)n_total, t->masked, t->offsets, t->d_totals, t->scan_temp,
+                                  &temp_bytes, s));
+            unsigned long long totals[2] = {0ull, 0ull};
+            TG_TRY(cudaMemcpyAsync(totals, t->d_totals, sizeof totals, cudaMemcpyDeviceToHost, s));
+            TG_TRY(cudaStreamSynchronize(s));
+            if (totals[1] == 0ull) {
+                float wave_ms = 0.0f;
+                TG_TRY(cudaEventElapsedTime(&wave_ms, t->ev_start, t->ev_stop));
+                t->kernel_ms += wave_ms;
+                t->waves += 1;
+                total = totals[0];
+                st = tracker_points(t, total, s);
+                if (st != TG_OK) return st;
+                TG_TRY(launch_gather(t->pool, t->chunk_next, t->first_chunk, t->lengths, t->offsets, nullptr,
+                                     (uint32_t)n_total, t->points, s));
+                t->launches += 1;
+                t->total_points = total;
+                TG_TRY(cudaMemcpyAsync(h_lengths, t->lengths, n_total * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                TG_TRY(cudaMemcpyAsync(h_offsets, t->offsets, n_total * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+                break;
+            }
+        }
         TG_TRY(cudaMemcpyAsync(t->h_len.data(), t->lengths, n_total * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         TG_TRY(cudaStreamSynchronize(s));
         float wave_ms = 0.0f;

@@ -228,6 +228,12 @@ cudaError_t launch_track_dense(const FieldDev& f, const TrackParams& p, const fl
                                float4* out, uint32_t* lengths, cudaStream_t stream);
 cudaError_t launch_track_persistent(const FieldDev& f, const PersistentParams& p, int grid,
                                     int block, cudaStream_t stream);
+// offsets[i] = exclusive prefix sum of the lengths, overflowed streamlines
+// counted as 0; totals[0] = points, totals[1] = overflowed streamlines.
+// With temp == nullptr, only sets *temp_bytes (scan scratch size).
+cudaError_t launch_offsets(const uint32_t* lengths, uint32_t n, uint64_t* masked, uint64_t* offsets,
+                           unsigned long long* totals, void* temp, size_t* temp_bytes, cudaStream_t stream);
+// seed_ids == nullptr: seeds 0..n_ids-1.
 cudaError_t launch_gather(const float* pool, const int32_t* chunk_next, const int32_t* first_chunk,
                           const uint32_t* lengths, const uint64_t* offsets, const uint32_t* seed_ids,
                           uint32_t n_ids, float* out_points, cudaStream_t stream);

@@ -24,6 +24,8 @@
  */
 #include <cuda_runtime.h>
 
+#include <cub/cub.cuh>
+
 #include "tg_internal.h"
 #include "tg_step.cuh"
 
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(256) gather_kernel(const float* __restrict__ p
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t k = warp; k < n_ids; k += n_warps) {
-        const uint32_t seed = seed_ids[k];
+        const uint32_t seed = seed_ids != nullptr ? seed_ids[k] : k;
         int32_t chunk = first_chunk[seed];
         const uint32_t len = lengths[seed];
         const uint64_t off = offsets[seed];
@@ -299,6 +301,38 @@ cudaError_t launch_gather(const float* pool, const int32_t* chunk_next, const in
     if (grid > (uint64_t)sms * 16) grid = (uint64_t)sms * 16;
     gather_kernel<<<(int)grid, block, 0, stream>>>(pool, chunk_next, first_chunk, lengths, offsets, seed_ids,
                                                    n_ids, out_points);
+    return cudaGetLastError();
+}
+
+// Lengths of streamlines that overflowed the pool count as 0; the count
+// of such streamlines goes to totals[1].
+__global__ void masked_lengths_kernel(const uint32_t* __restrict__ lengths, uint32_t n, uint64_t* __restrict__ out,
+                                      unsigned long long* __restrict__ totals)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool over = i < n && (lengths[i] & kOverflowBit) != 0u;
+    if (i < n) out[i] = over ? 0ull : (uint64_t)lengths[i];
+    const unsigned b = __ballot_sync(0xffffffffu, over);
+    if ((threadIdx.x & 31u) == 0u && b != 0u) atomicAdd(totals + 1, (unsigned long long)__popc(b));
+}
+
+__global__ void offsets_total_kernel(const uint64_t* __restrict__ masked, const uint64_t* __restrict__ offsets,
+                                     uint32_t n, unsigned long long* __restrict__ totals)
+{
+    totals[0] = offsets[n - 1] + masked[n - 1];
+}
+
+cudaError_t launch_offsets(const uint32_t* lengths, uint32_t n, uint64_t* masked, uint64_t* offsets,
+                           unsigned long long* totals, void* temp, size_t* temp_bytes, cudaStream_t stream)
+{
+    if (temp == nullptr) return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, masked, offsets, (int)n, stream);
+    cudaError_t e = cudaMemsetAsync(totals, 0, 2 * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess || n == 0) return e;
+    masked_lengths_kernel<<<(n + 255) / 256, 256, 0, stream>>>(lengths, n, masked, totals);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, masked, offsets, (int)n, stream);
+    if (e != cudaSuccess) return e;
+    offsets_total_kernel<<<1, 1, 0, stream>>>(masked, offsets, n, totals);
     return cudaGetLastError();
 }
 
