@@ -998,7 +998,8 @@ def run_serve(args):
             sweep.append({"rate_per_s": rate, "requests": n_req, "p50_s": float(np.percentile(lat, 50)),
                           "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
                           "steps": st.steps, "epochs": st.epochs, "busy_s": st.busy_seconds, "wall_s": wall,
-                          "kernel_s": st.kernel_seconds, "harvest_s": st.harvest_seconds,
+                          "kernel_s": st.kernel_seconds, "between_s": st.between_seconds,
+                          "harvest_s": st.harvest_seconds,
                           "steps_per_s": st.steps / max(1e-9, st.busy_seconds),
                           "streamlines_per_s": seeds_done / max(1e-9, st.busy_seconds),
                           "offered_seeds_per_s": float(offered / arrivals[-1])})

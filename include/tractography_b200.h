@@ -264,8 +264,11 @@ int tg_server_stats(const tg_server* server, uint64_t* steps, uint64_t* epochs, 
  * alone ends an epoch).  With a budget, every code path's lanes stop at the
  * same deadline, whatever their step cost; results do not change. */
 int tg_server_set_epoch_time(tg_server* server, double seconds);
-/* Device seconds spent in the epochs' tracking launches and in harvesting. */
-int tg_server_timing(const tg_server* server, double* kernel_seconds, double* harvest_seconds);
+/* Device-timeline seconds, summed over epochs: the tracking launches; from
+ * their end to the harvest's start (counter read-back and host bookkeeping);
+ * the harvest. */
+int tg_server_timing(const tg_server* server, double* kernel_seconds, double* between_seconds,
+                     double* harvest_seconds);
 
 /* Copy points [first, first + count) of the packed (total_points, 3)
  * float32 buffer of the last run to `dst` (host when dst_on_host != 0). */

@@ -164,7 +164,8 @@ def load() -> ctypes.CDLL:
                                   ctypes.c_int),
         "tg_server_take": ([P, U64, P, P, P], ctypes.c_int),
         "tg_server_set_epoch_time": ([P, ctypes.c_double], ctypes.c_int),
-        "tg_server_timing": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+        "tg_server_timing": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                              ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "tg_server_stats": ([P, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(ctypes.c_double),
                              ctypes.POINTER(U64)], ctypes.c_int),
         "tg_seeds_from_fod": ([I32, U32, P, P, U32, P, P, U32, P, P], ctypes.c_int),

@@ -40,6 +40,9 @@ struct tg_tracker {
     uint32_t* ids = nullptr;
     uint32_t* done_ids = nullptr;
     size_t cap_seeds = 0;
+    // closed-surface domain: the seeds' inside tests, done before tracking
+    uint8_t* seed_inside = nullptr;
+    size_t cap_seed_inside = 0;
     // device offsets of a run whose streamlines all fit the pool
     uint64_t* masked = nullptr;
     size_t cap_masked = 0;
@@ -486,6 +489,7 @@ int tg_tracker_destroy(tg_tracker* t)
     cudaFree(t->ids);
     cudaFree(t->done_ids);
     cudaFree(t->masked);
+    cudaFree(t->seed_inside);
     cudaFree(t->scan_temp);
     cudaFree(t->d_totals);
     cudaFree(t->seeds);
@@ -678,6 +682,14 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
     pp.chunk_counter = t->chunk_counter;
     pp.first_chunk = t->first_chunk;
     pp.lengths = t->lengths;
+    if (tp.domain_kind == kDomainMesh) {
+        // The inside test of a seed walks three long rays through the BVH.
+        // Inside the tracking kernel the lane that starts a streamline would
+        // hold its whole warp for those walks; a pre-pass (in the timed
+        // region) does them for every seed, with the same arithmetic.
+        TG_TRY(ensure(&t->seed_inside, &t->cap_seed_inside, n_seeds));
+        pp.seed_inside = t->seed_inside;
+    }
 
     const int block = persistent_block_size();
     int per_sm = persistent_blocks_per_sm(field->d, algorithm->algorithm, domain->d.kind);
@@ -707,6 +719,10 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
         pp.n_chunks = t->n_chunks;
         TG_TRY(cudaMemsetAsync(t->chunk_counter, 0, sizeof(unsigned int), s));
         TG_TRY(cudaEventRecord(t->ev_start, s));
+        if (first_wave && pp.seed_inside != nullptr) {
+            TG_TRY(launch_mesh_contains(tp.mesh, d_seeds, n_seeds, t->seed_inside, s, 2u));
+            t->launches += 1;
+        }
         // round 0 pulls seeds; rounds 1..R resume the streamlines handed over
         // by sparse warps of the previous round; the last round compacts no more
         for (uint32_t r = 0; r <= rounds; ++r) {

@@ -83,6 +83,7 @@ struct PersistentParams {
     uint32_t batch_size;
     const uint32_t* batch_rng_seeds;
     uint64_t seed_offset;         // Philox index base
+    const uint8_t* seed_inside;   // closed surface: per seed, the inside test done by a pre-pass; nullable
     unsigned long long* item_counter;
     // output: chunk pool
     float* pool;                  // n_chunks * kChunkPoints * 3 floats
@@ -219,8 +220,9 @@ cudaError_t launch_mesh_segments_blocked(const MeshDev& m, const float4* starts,
                                          uint8_t* blocked, cudaStream_t stream);
 cudaError_t launch_mesh_segment_hits(const MeshDev& m, const float4* starts, const float4* ends, uint32_t n,
                                      uint8_t* found, uint32_t* triangle, float4* hit, cudaStream_t stream);
+// Inside test of points[i * stride] (stride 2 for (n, 2) float4 seeds).
 cudaError_t launch_mesh_contains(const MeshDev& m, const float4* points, uint32_t n, uint8_t* out,
-                                 cudaStream_t stream);
+                                 cudaStream_t stream, uint32_t stride = 1);
 
 // Launchers (tg_track.cu).
 cudaError_t launch_track_dense(const FieldDev& f, const TrackParams& p, const float4* seeds,

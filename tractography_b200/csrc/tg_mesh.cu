@@ -417,11 +417,11 @@ __global__ void __launch_bounds__(128) mesh_segment_hits_kernel(MeshDev m, const
 }
 
 __global__ void __launch_bounds__(128) mesh_contains_kernel(MeshDev m, const float4* __restrict__ points,
-                                                            uint32_t n, uint8_t* __restrict__ out)
+                                                            uint32_t n, uint32_t stride, uint8_t* __restrict__ out)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float4 p = points[i];
+    const float4 p = points[(size_t)i * stride];
     out[i] = mesh_contains(m, p.x, p.y, p.z) ? 1 : 0;
 }
 
@@ -452,10 +452,10 @@ cudaError_t launch_mesh_segment_hits(const MeshDev& m, const float4* starts, con
 }
 
 cudaError_t launch_mesh_contains(const MeshDev& m, const float4* points, uint32_t n, uint8_t* out,
-                                 cudaStream_t stream)
+                                 cudaStream_t stream, uint32_t stride)
 {
     if (n == 0) return cudaSuccess;
-    mesh_contains_kernel<<<(n + 127) / 128, 128, 0, stream>>>(m, points, n, out);
+    mesh_contains_kernel<<<(n + 127) / 128, 128, 0, stream>>>(m, points, n, stride, out);
     return cudaGetLastError();
 }
 

@@ -76,6 +76,7 @@ struct ServeJob {
     uint64_t seed_offset;
     uint32_t* lengths;
     int32_t* first_chunk;
+    const uint8_t* seed_inside; // closed surface: the seeds' inside tests, done at admission; nullable
     unsigned int* counts;       // [0] streamlines in flight, [1] overflowed
     uint32_t chunks_needed;     // worst case per streamline: ceil(n_steps / 32)
     unsigned long long* finished_points;   // points of streamlines finished this epoch
@@ -227,6 +228,7 @@ __global__ void __launch_bounds__(128, 5) serve_kernel(const ServeParams sp)
             const float4 b = J->seeds[2 * (size_t)item + 1];
             const uint32_t batch = item / J->batch_size;
             lane_init(s, a, b, J->batch_rng_seeds[batch], item - batch * J->batch_size, J->seed_offset + item);
+            if (DOM == kDomainMesh && J->seed_inside != nullptr) s.seed_state = J->seed_inside[item] ? 1u : 2u;
             atomicAdd(J->counts, 1u);
             chunk = -1;
         }
@@ -451,6 +453,7 @@ struct ServeRequest {
     uint64_t reserve = 0;       // bytes counted against the budget while admitted
     // device (admitted)
     float4* d_seeds = nullptr;
+    uint8_t* d_inside = nullptr;
     uint32_t* d_rng = nullptr;
     uint32_t* d_lengths = nullptr;
     int32_t* d_first = nullptr;
@@ -515,8 +518,8 @@ struct tg_server {
     // device-clock epoch budget (0: epoch_steps only) and device timing
     uint64_t epoch_ns = 0;
     unsigned long long* d_deadline = nullptr;
-    cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr, ev_t2 = nullptr;
-    double kernel_s = 0.0, harvest_s = 0.0;
+    cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr, ev_t2 = nullptr, ev_t3 = nullptr;
+    double kernel_s = 0.0, harvest_s = 0.0, between_s = 0.0;
     // request buffers come from the server's own pool, which keeps freed
     // memory (up to the budget) for the next requests instead of returning
     // it to the driver at every synchronisation
@@ -541,10 +544,11 @@ int sfail_cuda(cudaError_t e, const char* what)
 
 void free_request_buffers(tg_server* S, ServeRequest* r)
 {
-    void* bufs[] = {r->d_seeds, r->d_rng, r->d_first, r->d_lengths, r->d_offset, r->d_result};
+    void* bufs[] = {r->d_seeds, r->d_inside, r->d_rng, r->d_first, r->d_lengths, r->d_offset, r->d_result};
     for (void* b : bufs)
         if (b) cudaFreeAsync(b, S->stream);
     r->d_seeds = nullptr;
+    r->d_inside = nullptr;
     r->d_rng = nullptr;
     r->d_first = nullptr;
     r->d_lengths = nullptr;
@@ -582,6 +586,12 @@ int admit(tg_server* S)
         // pageable copies are staged before cudaMemcpyAsync returns
         TG_STRY(cudaMemcpyAsync(r->d_seeds, r->host_seeds, (size_t)n * 32, cudaMemcpyHostToDevice, S->stream));
         TG_STRY(cudaMemcpyAsync(r->d_rng, r->host_rng, (size_t)r->n_batches * 4, cudaMemcpyHostToDevice, S->stream));
+        if (r->tp.domain_kind == kDomainMesh) {
+            // the seeds' inside tests (three ray walks each), done here for the
+            // whole request instead of by single lanes holding their warps
+            TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_inside), n, S->mempool, S->stream));
+            TG_STRY(launch_mesh_contains(r->tp.mesh, r->d_seeds, n, r->d_inside, S->stream, 2u));
+        }
         ServeJob& J = S->h_jobs[slot];
         std::memset(&J, 0, sizeof J);
         J.t = r->tp;
@@ -592,6 +602,7 @@ int admit(tg_server* S)
         J.seed_offset = r->job.algorithm.seed_offset;
         J.lengths = r->d_lengths;
         J.first_chunk = r->d_first;
+        J.seed_inside = r->d_inside;
         J.counts = S->d_counts + 2 * slot;
         J.finished_points = S->d_slot_points + 2 * slot;
         J.cursor = S->d_slot_points + 2 * slot + 1;
@@ -745,6 +756,7 @@ int tg_server_create(uint64_t hbm_budget_bytes, uint64_t pool_points, uint32_t e
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev_t0);
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev_t1);
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev_t2);
+    if (e == cudaSuccess) e = cudaEventCreate(&S->ev_t3);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->d_deadline), sizeof(unsigned long long));
     if (e == cudaSuccess) {
         cudaMemPoolProps props;
@@ -821,7 +833,7 @@ int tg_server_destroy(tg_server* S)
                     S->d_n_finished, S->d_deadline};
     for (void* b : bufs) cudaFree(b);
     if (S->mempool) cudaMemPoolDestroy(S->mempool);
-    cudaEvent_t evs[] = {S->ev_fork, S->ev_t0, S->ev_t1, S->ev_t2};
+    cudaEvent_t evs[] = {S->ev_fork, S->ev_t0, S->ev_t1, S->ev_t2, S->ev_t3};
     for (cudaEvent_t ev : evs)
         if (ev) cudaEventDestroy(ev);
     if (S->stream) cudaStreamDestroy(S->stream);
@@ -851,7 +863,7 @@ int tg_server_submit(tg_server* S, const tg_job* job, uint64_t* request_id)
     r->n_batches = n ? (n + job->batch_size - 1) / job->batch_size : 0;
     r->host_seeds = job->seeds;
     r->host_rng = job->batch_rng_seeds;
-    r->reserve = (uint64_t)n * 48 + (uint64_t)r->n_batches * 4 +
+    r->reserve = (uint64_t)n * 49 + (uint64_t)r->n_batches * 4 +
                  std::max<uint64_t>(1024, (uint64_t)n * std::min<uint64_t>(job->n_steps, S->points_estimate)) * 12;
     r->t_submit = now_s();
     *request_id = r->id;
@@ -1026,6 +1038,7 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
             }
             r->harvested += add;
         }
+        TG_STRY(cudaEventRecord(S->ev_t3, S->stream));
         if (n_fin > 0) {
             uint64_t g = ((uint64_t)n_fin * 32 + 255) / 256;
             if (g > (uint64_t)S->sms * 16) g = (uint64_t)S->sms * 16;
@@ -1070,9 +1083,10 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
         }
         TG_STRY(cudaStreamSynchronize(S->stream));
         S->busy_s += now_s() - t0;
-        float k_ms = 0.0f, h_ms = 0.0f;
+        float k_ms = 0.0f, b_ms = 0.0f, h_ms = 0.0f;
         if (cudaEventElapsedTime(&k_ms, S->ev_t0, S->ev_t1) == cudaSuccess) S->kernel_s += 1e-3 * k_ms;
-        if (cudaEventElapsedTime(&h_ms, S->ev_t1, S->ev_t2) == cudaSuccess) S->harvest_s += 1e-3 * h_ms;
+        if (cudaEventElapsedTime(&b_ms, S->ev_t1, S->ev_t3) == cudaSuccess) S->between_s += 1e-3 * b_ms;
+        if (cudaEventElapsedTime(&h_ms, S->ev_t3, S->ev_t2) == cudaSuccess) S->harvest_s += 1e-3 * h_ms;
         st = admit(S);
         if (st != TG_OK) return st;
     }
@@ -1130,10 +1144,11 @@ int tg_server_set_epoch_time(tg_server* S, double seconds)
     return TG_OK;
 }
 
-int tg_server_timing(const tg_server* S, double* kernel_seconds, double* harvest_seconds)
+int tg_server_timing(const tg_server* S, double* kernel_seconds, double* between_seconds, double* harvest_seconds)
 {
     if (S == nullptr) return sfail(TG_ERR_INVALID_ARGUMENT, "server is null");
     if (kernel_seconds) *kernel_seconds = S->kernel_s;
+    if (between_seconds) *between_seconds = S->between_s;
     if (harvest_seconds) *harvest_seconds = S->harvest_s;
     return TG_OK;
 }

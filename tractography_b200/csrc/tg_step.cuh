@@ -28,8 +28,11 @@ struct Lane {
     float dvx, dvy, dvz;
     float fvx, fvy, fvz;
     uint32_t steps;
-    // closed-surface domain: the point of the last passed domain test
+    // closed-surface domain: the point of the last passed domain test, and
+    // the seed's inside test when a pre-pass computed it (0: not known, test
+    // here; 1: inside; 2: outside)
     float lx, ly, lz;
+    uint32_t seed_state;
 };
 
 // One iteration of tracking.py:121-147 after the n < N_STEPS test.
@@ -49,7 +52,8 @@ __device__ __forceinline__ bool locate(const TrackParams& p, Lane& s, float (&c)
     float ax, ay, az;
     if constexpr (DOM == kDomainMesh) {
         if (s.steps == 0u) {
-            if (!mesh_contains(p.mesh, s.px, s.py, s.pz)) return false;
+            const bool inside = s.seed_state == 0u ? mesh_contains(p.mesh, s.px, s.py, s.pz) : s.seed_state == 1u;
+            if (!inside) return false;
         } else if (mesh_segment_blocked(p.mesh, s.lx, s.ly, s.lz, s.px, s.py, s.pz)) {
             return false;
         }
@@ -247,6 +251,7 @@ __device__ __forceinline__ void lane_restore(Lane& s, const LaneCarry& c, uint32
     s.rng.index = c.rng_index;
     s.dvx = s.dvy = s.dvz = __int_as_float(0x7fc00000);
     s.fvx = s.fvy = s.fvz = __int_as_float(0x7fc00000);
+    s.seed_state = 0u;
     chunk = c.chunk;
     fill = c.fill;
 }
@@ -275,6 +280,7 @@ __device__ __forceinline__ void lane_init(Lane& s, float4 a, float4 b, uint32_t 
     s.lx = a.x;
     s.ly = a.y;
     s.lz = a.z;
+    s.seed_state = 0u;
 }
 
 }  // namespace tg

@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(128, 5) track_persistent_kernel(const Persiste
             const uint32_t batch = item / pp.batch_size;
             const uint32_t local = item - batch * pp.batch_size;
             lane_init(s, a, b, pp.batch_rng_seeds[batch], local, pp.seed_offset + item);
+            if (DOM == kDomainMesh && pp.seed_inside != nullptr) s.seed_state = pp.seed_inside[item] ? 1u : 2u;
             if (!chunk_alloc(pp, chunk)) {
                 pp.first_chunk[item] = -1;
                 pp.lengths[item] = kOverflowBit;

@@ -35,6 +35,7 @@ class ServerStats:
     busy_seconds: float          # host wall time of the epochs
     reserved_bytes: int
     kernel_seconds: float = 0.0  # device time of the epochs' tracking launches
+    between_seconds: float = 0.0 # from their end to the harvest (read-back, host bookkeeping)
     harvest_seconds: float = 0.0 # device time of moving finished streamlines to their results
 
 
@@ -152,9 +153,11 @@ class Server:
         steps, epochs, busy, reserved = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double(), ctypes.c_uint64()
         _lib.check(self.lib.tg_server_stats(self._handle, ctypes.byref(steps), ctypes.byref(epochs),
                                             ctypes.byref(busy), ctypes.byref(reserved)))
-        kernel, harvest = ctypes.c_double(), ctypes.c_double()
-        _lib.check(self.lib.tg_server_timing(self._handle, ctypes.byref(kernel), ctypes.byref(harvest)))
-        return ServerStats(steps.value, epochs.value, busy.value, reserved.value, kernel.value, harvest.value)
+        kernel, between, harvest = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.lib.tg_server_timing(self._handle, ctypes.byref(kernel), ctypes.byref(between),
+                                             ctypes.byref(harvest)))
+        return ServerStats(steps.value, epochs.value, busy.value, reserved.value, kernel.value, between.value,
+                           harvest.value)
 
     def drain(self) -> dict:
         """Poll until every submitted request finished; returns {id: Tractogram}."""
