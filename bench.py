@@ -77,7 +77,8 @@ def parse_args():
     p.add_argument("--seeds", type=int, default=1000000, help="seeds per step (one tg.tractogram job)")
     p.add_argument("--batch", type=int, default=50000, help="reference batch_size inside a job")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["config1", "config0", "mixed", "config2", "serve"], default="config1",
+    p.add_argument("--workload", choices=["config1", "config0", "mixed", "config2", "serve", "tod", "connectome"],
+                   default="config1",
                    help="config1 (default headline), the 64-job mixed workload, the DTI + mesh workload, or "
                         "serving under Poisson load")
     p.add_argument("--rates", default="5,20,50,100,200", help="serving: arrival rates (requests/s)")
@@ -670,6 +671,137 @@ def run_mixed(args):
     print(json.dumps(line), flush=True)
 
 
+PRODUCT_SEEDS = 100000
+PRODUCT_WORKLOAD = ("{kind} on the config-1 volume: SH lmax 8 (45 f32 coefficients) 145x174x145 at 1.25 mm, 3 "
+                    "bundles; domain = nonzero voxels (the whole box); {n} boundary seeds (domain.seed's sampler) "
+                    "per step; the reference's default algorithm for tg.{kind} (Transport, step 0.001 mm, gamma 1); "
+                    "maximum length 300 mm{extra}")
+
+
+def run_product(args):
+    """TOD or connectome (tracking.py:181-385, :388-602) on the config-1 volume."""
+    import torch
+
+    import tractography_b200 as tg
+    from tractography_b200 import _lib, synthetic, tracking
+    from tractography_b200.algorithm import to_struct
+
+    kind = args.workload
+    torch.cuda.set_device(0)
+    runtime = tg.CudaRuntime(0)
+    lib = runtime.lib
+    sh = ctypes.c_void_p(runtime.stream_handle)
+    fod = synthetic.config1(seed=0)
+    field = tg.field.Image(fod)
+    mask = np.any(field.values != 0, axis=-1).astype(np.uint8)
+    domain = tg.domain.Image(tg.Nifti1Image(mask, fod.affine))
+    n_seeds = args.seeds if args.seeds != 1000000 else PRODUCT_SEEDS
+    model = tg.local.RealSymmetricSphericalHarmonics(C)
+    algorithm = tg.algorithm.Transport(model)                 # step 0.001, gamma 1 (the reference defaults)
+    n_steps = int(math.floor(MAX_LENGTH / algorithm.step_size))
+    v4, f4, cumulative = domain.boundary_arrays()
+    shape = fod.shape[:3]
+    inv = np.ascontiguousarray(np.linalg.inv(np.asarray(fod.affine, np.float64)), dtype=np.float32)
+    with runtime.device_scope():
+        d_h, f_h = tracking._handles(algorithm, domain, field, runtime)
+        b_h = domain.boundary_bvh().device(runtime) if kind == "connectome" else None
+        dv, df, dc = runtime.to_device(v4), runtime.to_device(f4), runtime.to_device(cumulative)
+        steps = torch.zeros((1,), dtype=torch.int64, device=runtime.device)
+        if kind == "tod":
+            out = torch.zeros(tuple(shape) + (45,), dtype=torch.float32, device=runtime.device)
+            dims = np.asarray(shape, dtype=np.uint32)
+        else:
+            rows = runtime.empty((9 * n_seeds,), torch.int32)
+            cols = runtime.empty((9 * n_seeds,), torch.int32)
+            weights = runtime.empty((9 * n_seeds,), torch.float32)
+
+        def run(rng_seed):
+            a = to_struct(algorithm, rng_seed)
+            if kind == "tod":
+                out.zero_()
+                _lib.check(lib.tg_tod(ctypes.byref(a), d_h, f_h, ctypes.c_void_p(dv.data_ptr()), len(v4),
+                                      ctypes.c_void_p(df.data_ptr()), ctypes.c_void_p(dc.data_ptr()), len(f4),
+                                      n_seeds, n_steps, dims.ctypes.data_as(ctypes.c_void_p),
+                                      inv.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(out.data_ptr()),
+                                      ctypes.c_void_p(steps.data_ptr()), sh))
+            else:
+                _lib.check(lib.tg_connectome(ctypes.byref(a), d_h, f_h, b_h, ctypes.c_void_p(dv.data_ptr()), len(v4),
+                                             ctypes.c_void_p(df.data_ptr()), ctypes.c_void_p(dc.data_ptr()), len(f4),
+                                             n_seeds, n_steps, 0.0, ctypes.c_void_p(rows.data_ptr()),
+                                             ctypes.c_void_p(cols.data_ptr()), ctypes.c_void_p(weights.data_ptr()),
+                                             ctypes.c_void_p(steps.data_ptr()), sh))
+
+        for w in range(args.warmup):
+            run(1000 + w)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(0)
+        with sampler:
+            torch.cuda.synchronize()
+            steps.zero_()
+            ev0.record(runtime.stream)
+            for k in range(args.steps):
+                run(k)
+            ev1.record(runtime.stream)
+            torch.cuda.synchronize()
+            dev_ms = ev0.elapsed_time(ev1)
+            dev_steps = int(steps.item())
+            # end to end: the public call (host arrays out: the TOD image / the CSR matrix)
+            e2e_steps, t0 = 0, time.perf_counter()
+            for k in range(args.steps):
+                st = {}
+                if kind == "tod":
+                    tracking.tod(algorithm, domain, field, fod, n_seeds, runtime=runtime, stats=st)
+                else:
+                    tracking.connectome(algorithm, domain, field, n_seeds, runtime=runtime, stats=st)
+                e2e_steps += st["steps"]
+            torch.cuda.synchronize()
+            e2e_s = time.perf_counter() - t0
+    out_bytes = int(np.prod(shape)) * 45 * 4 if kind == "tod" else 9 * n_seeds * 12
+    line = {"metric": METRIC, "value": dev_steps / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator; no dataset)",
+            "workload": kind,
+            "config": {"workload": PRODUCT_WORKLOAD.format(
+                kind=kind, n=n_seeds,
+                extra="; output: the (145, 174, 145, 45) raw TOD on the field grid" if kind == "tod" else
+                "; output: 9 weighted contributions per track (end segment hit on the boundary BVH)"),
+                "boundary_triangles": len(f4)},
+            "tracks_per_s": n_seeds * args.steps / (dev_ms / 1e3),
+            "e2e": {"value": e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": out_bytes,
+                    "note": "wall clock of the public tracking call; boundary arrays resident"},
+            "gpu_launches": args.steps, "clocks": sampler.summary()}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        threads = os.cpu_count() or 1
+        n_cpu = max(8 * threads, 64)
+        case = O.Case(mask=domain.values, mask_inv_affine=domain.inverse_affine, field=field.values,
+                      field_inv_affine=field.inverse_affine, step_size=algorithm.step_size, gamma=1.0, rng_seed=7)
+        t0 = time.perf_counter()
+        if kind == "tod":
+            case.tod((v4, f4, cumulative), n_cpu, n_steps, shape, inv)
+        else:
+            bvh = O.BoundaryBvh.build(domain.boundary.vertices, domain.boundary.faces)
+            t0 = time.perf_counter()
+            case.connectome(bvh, (v4, f4, cumulative), n_cpu, n_steps)
+        dt = time.perf_counter() - t0
+        # steps of the sample: the same tracks on the GPU (bit-identical loop)
+        with runtime.device_scope():
+            a = to_struct(algorithm, 7)
+            steps.zero_()
+            n_save = n_seeds
+            n_seeds = n_cpu
+            run(7)
+            n_seeds = n_save
+            torch.cuda.synchronize()
+            cpu_steps = int(steps.item())
+        line["cpu_baseline"] = {"value": cpu_steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{n_cpu} tracks ({cpu_steps} steps, {dt:.1f} s); plain-C oracle, "
+                                          f"OpenMP over tracks"}
+    print(json.dumps(line), flush=True)
+
+
 C0_WORKLOAD = ("config0 Transport: SH lmax 8 (45 f32 coefficients) 32^3 at 2 mm, bundle along x and y-z arcs, "
                "ellipsoid mask 14/12/12 voxels; 10000 seeds uniform in the mask; step 0.2 mm (0.1 voxel), gamma 1; "
                "save_at 0.25, max length 300 mm")
@@ -1026,6 +1158,8 @@ def main():
         run_config2(args)
     elif args.workload == "config0":
         run_config0(args)
+    elif args.workload in ("tod", "connectome"):
+        run_product(args)
     elif args.workload == "serve":
         run_serve(args)
     else:

@@ -322,11 +322,13 @@ int tg_field_evaluate(const tg_field* field, const float* points, uint32_t n, fl
  * is added into `coefficients`, a device (out_dims[0], out_dims[1],
  * out_dims[2], 45) float32 array (not cleared; the caller zeroes it), at the
  * voxel floor(A^-1 p + 0.5) of the output grid (out_inverse_affine,
- * row-major 4x4).  Additions from different threads are unordered. */
+ * row-major 4x4).  Additions from different threads are unordered.
+ * steps (nullable, device uint64): the iterations that passed the domain and
+ * field tests are added to it. */
 int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field, const float* vertices,
            uint32_t n_vertices, const uint32_t* triangles, const float* cumulative_areas, uint32_t n_triangles,
            uint32_t n_seeds, uint32_t n_steps, const uint32_t out_dims[3], const float out_inverse_affine[16],
-           float* coefficients, void* stream);
+           float* coefficients, uint64_t* steps, void* stream);
 /* tracking.connectome (tracking.py:388-602): n_seeds boundary seeds
  * (sampler arrays as for tg_boundary_seeds) tracked for at most n_steps
  * iterations; a track that moved at least minimum_length and whose final
@@ -334,11 +336,13 @@ int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_fiel
  * from the same vertices and faces) writes the 9 products of its start and
  * end barycentric weights at (start vertex, end vertex) pairs into rows,
  * columns and weights (device, 9 per seed; rows = -1 where nothing was
- * written).  Deterministic. */
+ * written).  Deterministic.  steps (nullable, device uint64) as for
+ * tg_tod. */
 int tg_connectome(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
                   const tg_domain* boundary, const float* vertices, uint32_t n_vertices, const uint32_t* triangles,
                   const float* cumulative_areas, uint32_t n_triangles, uint32_t n_seeds, uint32_t n_steps,
-                  float minimum_length, int32_t* rows, int32_t* columns, float* weights, void* stream);
+                  float minimum_length, int32_t* rows, int32_t* columns, float* weights, uint64_t* steps,
+                  void* stream);
 /* domain.seed, domain.py:494-575 with domain_sample_boundary (:95-120):
  * n_seeds seeds uniform over a boundary surface's area, pointing inward,
  * seed i drawing from rng_init(rng_seed, i).  Device arrays: vertices

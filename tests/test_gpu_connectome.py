@@ -29,10 +29,14 @@ def _device_contributions(alg, domain, field, n_seeds, n_steps, min_len, runtime
         rows = runtime.empty((9 * n_seeds,), torch.int32)
         cols = runtime.empty((9 * n_seeds,), torch.int32)
         w = runtime.empty((9 * n_seeds,), torch.float32)
+        steps = torch.zeros((1,), dtype=torch.int64, device=runtime.device)
         _lib.check(runtime.lib.tg_connectome(
             ctypes.byref(a), d_h, f_h, b_h, ctypes.c_void_p(dv.data_ptr()), len(v4), ctypes.c_void_p(df.data_ptr()),
             ctypes.c_void_p(dc.data_ptr()), len(f4), n_seeds, n_steps, min_len, ctypes.c_void_p(rows.data_ptr()),
-            ctypes.c_void_p(cols.data_ptr()), ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(runtime.stream_handle)))
+            ctypes.c_void_p(cols.data_ptr()), ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(steps.data_ptr()),
+            ctypes.c_void_p(runtime.stream_handle)))
+        # the step counter: every track takes at most n_steps steps, and some take steps
+        assert 0 < int(steps.item()) <= n_seeds * n_steps
         return rows.cpu().numpy(), cols.cpu().numpy(), w.cpu().numpy()
 
 

@@ -172,8 +172,8 @@ def load() -> ctypes.CDLL:
         "tg_domain_contains": ([P, P, U32, P, P], ctypes.c_int),
         "tg_field_evaluate": ([P, P, U32, P, P], ctypes.c_int),
         "tg_boundary_seeds": ([P, U32, P, P, U32, U32, U32, P, P], ctypes.c_int),
-        "tg_tod": ([AP, P, P, P, U32, P, P, U32, U32, U32, P, P, P, P], ctypes.c_int),
-        "tg_connectome": ([AP, P, P, P, P, U32, P, P, U32, U32, U32, F, P, P, P, P], ctypes.c_int),
+        "tg_tod": ([AP, P, P, P, U32, P, P, U32, U32, U32, P, P, P, P, P], ctypes.c_int),
+        "tg_connectome": ([AP, P, P, P, P, U32, P, P, U32, U32, U32, F, P, P, P, P, P], ctypes.c_int),
         "tg_local_evaluate": ([I32, U32, P, P, U32, P, P], ctypes.c_int),
         "tg_update_orientation": ([I32, U32, AP, P, P, U32, P, P], ctypes.c_int),
         "tg_rng_stream": ([I32, U32, U32, U32, U32, P, P], ctypes.c_int),

@@ -1193,7 +1193,7 @@ int tg_boundary_seeds(const float* vertices, uint32_t n_vertices, const uint32_t
 int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field, const float* vertices,
            uint32_t n_vertices, const uint32_t* triangles, const float* cumulative_areas, uint32_t n_triangles,
            uint32_t n_seeds, uint32_t n_steps, const uint32_t out_dims[3], const float out_inverse_affine[16],
-           float* coefficients, void* stream)
+           float* coefficients, uint64_t* steps, void* stream)
 {
     TodParams q;
     std::memset(&q, 0, sizeof q);
@@ -1221,6 +1221,7 @@ int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_fiel
     q.ny = out_dims[1];
     q.nz = out_dims[2];
     q.coefficients = coefficients;
+    q.steps = reinterpret_cast<unsigned long long*>(steps);
     TG_TRY(launch_tod(field->d.model, field->d.lmax, q, as_stream(stream)));
     return TG_OK;
 }
@@ -1228,7 +1229,8 @@ int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_fiel
 int tg_connectome(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
                   const tg_domain* boundary, const float* vertices, uint32_t n_vertices, const uint32_t* triangles,
                   const float* cumulative_areas, uint32_t n_triangles, uint32_t n_seeds, uint32_t n_steps,
-                  float minimum_length, int32_t* rows, int32_t* columns, float* weights, void* stream)
+                  float minimum_length, int32_t* rows, int32_t* columns, float* weights, uint64_t* steps,
+                  void* stream)
 {
     ConnectomeParams q;
     std::memset(&q, 0, sizeof q);
@@ -1257,6 +1259,7 @@ int tg_connectome(const tg_algorithm* algorithm, const tg_domain* domain, const 
     q.rows = rows;
     q.columns = columns;
     q.weights = weights;
+    q.steps = reinterpret_cast<unsigned long long*>(steps);
     TG_TRY(launch_connectome(field->d.model, field->d.lmax, q, as_stream(stream)));
     return TG_OK;
 }

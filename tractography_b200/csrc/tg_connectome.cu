@@ -60,6 +60,7 @@ __global__ void __launch_bounds__(128) connectome_kernel(const ConnectomeParams 
         s.pz = fmaf(h, s.oz, s.pz);
         tracked += 1u;
     }
+    add_steps(q.steps, s.steps);
     if ((float)tracked * p.algo.step_size < q.minimum_length) return;
     const Segment g = make_segment(qx, qy, qz, s.px, s.py, s.pz);
     float t, u = 0.0f, v = 0.0f;

@@ -174,6 +174,7 @@ struct TodParams {
     float4 out_row0, out_row1, out_row2;   // output grid inverse affine rows
     uint32_t nx, ny, nz;
     float* coefficients;           // (nx, ny, nz, 45) float32, accumulated
+    unsigned long long* steps;     // nullable: loop iterations that passed the domain and field tests
 };
 cudaError_t launch_tod(int model, int lmax, const TodParams& q, cudaStream_t stream);
 
@@ -193,6 +194,7 @@ struct ConnectomeParams {
     int32_t* rows;                 // 9 per seed, -1 when the track contributes nothing
     int32_t* columns;
     float* weights;
+    unsigned long long* steps;     // nullable: loop iterations that passed the domain and field tests
 };
 cudaError_t launch_connectome(int model, int lmax, const ConnectomeParams& q, cudaStream_t stream);
 

@@ -256,6 +256,16 @@ __device__ __forceinline__ void lane_restore(Lane& s, const LaneCarry& c, uint32
     fill = c.fill;
 }
 
+// Adds the steps of the calling lanes (those still running) to *total, one
+// atomic per warp.
+__device__ __forceinline__ void add_steps(unsigned long long* total, uint32_t steps)
+{
+    if (total == nullptr) return;
+    const unsigned mask = __activemask();
+    const uint32_t sum = __reduce_add_sync(mask, steps);
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(mask) - 1)) atomicAdd(total, (unsigned long long)sum);
+}
+
 // Tail compaction rule, evaluated by whole warps: once a lane of the warp
 // has found its queue empty (so the warp is not full), a warp with at most
 // `compact_lanes` live lanes hands them to the next round and exits.

@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(kTodThreads) tod_kernel(const TodParams q)
         s.pz = fmaf(h, s.oz, s.pz);
     }
     if (prev_x >= 0) tod_flush(q.coefficients, acc, tid, prev_x, prev_y, prev_z, q);
+    add_steps(q.steps, s.steps);
 }
 
 template <int M, int L, int A, int D>

@@ -164,7 +164,7 @@ def tractogram_dense(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseFi
 
 
 def tod(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, image, n_seeds: int,
-        maximum_streamline_length: float = 300.0, runtime=None):
+        maximum_streamline_length: float = 300.0, runtime=None, *, stats: dict | None = None):
     """Track orientation distribution as lmax-8 SH coefficients (tracking.py:181-385).
 
     ``n_seeds`` seeds are drawn on the domain boundary (``domain.seed``'s
@@ -173,7 +173,9 @@ def tod(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, image, n
     floor(maximum_streamline_length / step_size) iterations and the real SH
     basis of its orientation at every iteration is added to the output voxel
     nearest the point on ``image``'s grid.  Each nonempty voxel is normalised
-    to unit integral.  Returns an image of shape image.shape + (45,).
+    to unit integral.  Returns an image of shape image.shape + (45,).  When
+    ``stats`` is a dict, stats["steps"] receives the number of tracking
+    iterations that passed the domain and field tests.
     """
     from .nifti import Nifti1Image
     from .utils import normalize_odf
@@ -206,19 +208,24 @@ def tod(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, image, n
                           algorithm.philox_key() if algorithm.rng_mode() == _lib.RNG_PHILOX else 0, 0)
             dv, df, dc = runtime.to_device(v4), runtime.to_device(f4), runtime.to_device(cumulative)
             coefficients = torch.zeros(output_shape + (45,), dtype=torch.float32, device=runtime.device)
+            steps = torch.zeros((1,), dtype=torch.int64, device=runtime.device)
             dims = np.asarray(output_shape, dtype=np.uint32)
             _lib.check(runtime.lib.tg_tod(
                 ctypes.byref(a), d_handle, f_handle, ctypes.c_void_p(dv.data_ptr()), len(v4),
                 ctypes.c_void_p(df.data_ptr()), ctypes.c_void_p(dc.data_ptr()), len(f4), int(n_seeds), n_steps,
                 dims.ctypes.data_as(ctypes.c_void_p), inverse_affine.ctypes.data_as(ctypes.c_void_p),
-                ctypes.c_void_p(coefficients.data_ptr()), ctypes.c_void_p(runtime.stream_handle)))
+                ctypes.c_void_p(coefficients.data_ptr()), ctypes.c_void_p(steps.data_ptr()),
+                ctypes.c_void_p(runtime.stream_handle)))
             raw = coefficients.cpu().numpy()
+            if stats is not None:
+                stats["steps"] = int(steps.item())
     header = getattr(image, "header", None)
     return Nifti1Image(normalize_odf(raw).astype(np.float32), affine, header)
 
 
 def connectome(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, n_seeds: int,
-               maximum_streamline_length: float = 300.0, minimum_streamline_length: float = 0.0, runtime=None):
+               maximum_streamline_length: float = 300.0, minimum_streamline_length: float = 0.0, runtime=None, *,
+               stats: dict | None = None):
     """Directed piecewise-linear boundary connectome (tracking.py:388-602).
 
     Tracks start on the domain boundary (``domain.seed``'s sampler); when a
@@ -227,6 +234,7 @@ def connectome(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, n
     and hit the boundary adds the outer product of its start and end
     barycentric weights at the two triangles' vertices.  Returns a float32
     (n_vertices, n_vertices) CSR matrix over ``domain.boundary.vertices``.
+    ``stats`` as for :func:`tod`.
     """
     from scipy.sparse import coo_matrix, csr_matrix
 
@@ -263,12 +271,16 @@ def connectome(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, n
         rows = runtime.empty((9 * int(n_seeds),), torch.int32)
         cols = runtime.empty((9 * int(n_seeds),), torch.int32)
         weights = runtime.empty((9 * int(n_seeds),), torch.float32)
+        steps = torch.zeros((1,), dtype=torch.int64, device=runtime.device)
         _lib.check(runtime.lib.tg_connectome(
             ctypes.byref(a), d_handle, f_handle, b_handle, ctypes.c_void_p(dv.data_ptr()), len(v4),
             ctypes.c_void_p(df.data_ptr()), ctypes.c_void_p(dc.data_ptr()), len(f4), int(n_seeds), n_steps,
             float(minimum_streamline_length), ctypes.c_void_p(rows.data_ptr()), ctypes.c_void_p(cols.data_ptr()),
-            ctypes.c_void_p(weights.data_ptr()), ctypes.c_void_p(runtime.stream_handle)))
+            ctypes.c_void_p(weights.data_ptr()), ctypes.c_void_p(steps.data_ptr()),
+            ctypes.c_void_p(runtime.stream_handle)))
         rows, cols, weights = rows.cpu().numpy(), cols.cpu().numpy(), weights.cpu().numpy()
+        if stats is not None:
+            stats["steps"] = int(steps.item())
     return contributions_to_matrix(rows, cols, weights, n_vertices)
 
 
