@@ -613,6 +613,7 @@ def run_mixed(args):
             torch.cuda.synchronize()
             q_ms += ev0.elapsed_time(ev1)
         plain_len = d_len.cpu().numpy().view(np.uint32)
+        same_lengths = bool(np.array_equal(plain_len, lengths))
         work = int(steps.value)
         persistent_kernel_ms = float(kms.value)
         persistent_launches = int(launches.value)
@@ -657,7 +658,7 @@ def run_mixed(args):
         "gpu_launches_per_step": persistent_launches,
         "kernel_ms_per_step": persistent_kernel_ms,
         "plain_launches_per_step": n_plain,
-        "identical_lengths": bool(np.array_equal(plain_len, lengths)),
+        "identical_lengths": same_lengths,
         "config": {
             "workload": ("64 jobs: volume 64^3 / 96x96x60 / 128^3 / 145x174x145, SH lmax 4/6/8, seeds "
                          "log-U[1k, 500k], Transport or Diffusion (noise U[0.05, 0.2]), max length "
@@ -1103,24 +1104,35 @@ def run_serve(args):
             server = Server(runtime, hbm_budget_bytes=150e9 - resident, pool_points=256 << 20,
                             epoch_steps=args.epoch_steps, epoch_seconds=args.epoch_ms * 1e-3, max_requests=128)
             latency, seeds_done = [], 0
+            client = {"prepare_s": 0.0, "submit_s": 0.0, "poll_s": 0.0, "take_s": 0.0, "idle_s": 0.0}
             t0 = time.perf_counter()
             submitted = 0
             while len(latency) < n_req:
                 now = time.perf_counter() - t0
                 while submitted < n_req and arrivals[submitted] <= now:
+                    c0 = time.perf_counter()
                     job = make_request(volumes, rng)
+                    c1 = time.perf_counter()
                     offered += job.n_seeds
                     server.submit(job)
+                    client["prepare_s"] += c1 - c0
+                    client["submit_s"] += time.perf_counter() - c1
                     submitted += 1
+                c0 = time.perf_counter()
                 finished = server.poll()
+                c1 = time.perf_counter()
+                client["poll_s"] += c1 - c0
                 for rid in finished:
                     _, _, lengths, seconds = server.take(rid, points=False)
                     latency.append(seconds)
                     seeds_done += len(lengths)
+                client["take_s"] += time.perf_counter() - c1
                 if not finished and server.active == 0 and server.pending == 0:
                     if submitted == n_req:
                         raise RuntimeError("the server holds no work but requests are unfinished")
+                    c0 = time.perf_counter()
                     time.sleep(max(0.0, min(0.002, arrivals[submitted] - (time.perf_counter() - t0))))
+                    client["idle_s"] += time.perf_counter() - c0
                 if time.perf_counter() - t0 > 600.0:
                     raise RuntimeError(f"rate {rate}: requests still unfinished after 600 s")
             wall = time.perf_counter() - t0
@@ -1130,6 +1142,7 @@ def run_serve(args):
             sweep.append({"rate_per_s": rate, "requests": n_req, "p50_s": float(np.percentile(lat, 50)),
                           "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
                           "steps": st.steps, "epochs": st.epochs, "busy_s": st.busy_seconds, "wall_s": wall,
+                          "client": client,
                           "kernel_s": st.kernel_seconds, "between_s": st.between_seconds,
                           "harvest_s": st.harvest_seconds,
                           "steps_per_s": st.steps / max(1e-9, st.busy_seconds),

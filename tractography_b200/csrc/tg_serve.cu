@@ -524,6 +524,8 @@ struct tg_server {
     // memory (up to the budget) for the next requests instead of returning
     // it to the driver at every synchronisation
     cudaMemPool_t mempool = nullptr;
+    // pinned host block for the per-epoch read-back of counters
+    unsigned char* h_readback = nullptr;
 };
 
 namespace {
@@ -714,7 +716,7 @@ int requeue_overflow(tg_server* S, int slot)
 int grow_result(tg_server* S, int slot, uint64_t need)
 {
     ServeRequest* r = S->slots[slot];
-    uint64_t cap = std::max<uint64_t>(need, r->result_cap + r->result_cap / 2);
+    uint64_t cap = std::max<uint64_t>(need, 2 * r->result_cap);
     float* fresh = nullptr;
     TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&fresh), cap * 12, S->mempool, S->stream));
     if (r->harvested > 0)
@@ -758,6 +760,10 @@ int tg_server_create(uint64_t hbm_budget_bytes, uint64_t pool_points, uint32_t e
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev_t2);
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev_t3);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&S->d_deadline), sizeof(unsigned long long));
+    if (e == cudaSuccess)
+        e = cudaMallocHost(reinterpret_cast<void**>(&S->h_readback),
+                           kServeKinds * (sizeof(unsigned long long) + sizeof(unsigned int)) +
+                               (size_t)max_requests * 2 * (sizeof(unsigned int) + sizeof(unsigned long long)) + 64);
     if (e == cudaSuccess) {
         cudaMemPoolProps props;
         std::memset(&props, 0, sizeof props);
@@ -833,6 +839,7 @@ int tg_server_destroy(tg_server* S)
                     S->d_n_finished, S->d_deadline};
     for (void* b : bufs) cudaFree(b);
     if (S->mempool) cudaMemPoolDestroy(S->mempool);
+    if (S->h_readback) cudaFreeHost(S->h_readback);
     cudaEvent_t evs[] = {S->ev_fork, S->ev_t0, S->ev_t1, S->ev_t2, S->ev_t3};
     for (cudaEvent_t ev : evs)
         if (ev) cudaEventDestroy(ev);
@@ -1009,21 +1016,26 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
         TG_STRY(cudaEventRecord(S->ev_t1, S->stream));
         pool_settle_kernel<<<1, 1, 0, S->stream>>>(S->P.alloc);
         TG_STRY(cudaGetLastError());
-        unsigned long long counter[kServeKinds];
-        unsigned int carry_count[kServeKinds];
-        unsigned int n_fin = 0;
-        std::vector<unsigned int> counts(2 * S->max_slots);
-        std::vector<unsigned long long> slot_points(2 * S->max_slots);
-        unsigned long long steps = 0;
-        TG_STRY(cudaMemcpyAsync(counter, S->d_counter, sizeof counter, cudaMemcpyDeviceToHost, S->stream));
-        TG_STRY(cudaMemcpyAsync(carry_count, S->d_carry_count, sizeof carry_count, cudaMemcpyDeviceToHost, S->stream));
-        TG_STRY(cudaMemcpyAsync(counts.data(), S->d_counts, counts.size() * sizeof(unsigned int),
+        // read-back into one pinned block (asynchronous copies, one synchronisation)
+        unsigned long long* const slot_points = reinterpret_cast<unsigned long long*>(S->h_readback);
+        unsigned long long* const counter = slot_points + 2 * (size_t)S->max_slots;
+        unsigned long long* const steps_p = counter + kServeKinds;
+        unsigned int* const counts = reinterpret_cast<unsigned int*>(steps_p + 1);
+        unsigned int* const carry_count = counts + 2 * (size_t)S->max_slots;
+        unsigned int* const n_fin_p = carry_count + kServeKinds;
+        TG_STRY(cudaMemcpyAsync(counter, S->d_counter, kServeKinds * sizeof(unsigned long long),
                                 cudaMemcpyDeviceToHost, S->stream));
-        TG_STRY(cudaMemcpyAsync(slot_points.data(), S->d_slot_points, slot_points.size() * sizeof(unsigned long long),
+        TG_STRY(cudaMemcpyAsync(carry_count, S->d_carry_count, kServeKinds * sizeof(unsigned int),
                                 cudaMemcpyDeviceToHost, S->stream));
-        TG_STRY(cudaMemcpyAsync(&n_fin, S->d_n_finished, sizeof n_fin, cudaMemcpyDeviceToHost, S->stream));
-        TG_STRY(cudaMemcpyAsync(&steps, S->d_steps, sizeof steps, cudaMemcpyDeviceToHost, S->stream));
+        TG_STRY(cudaMemcpyAsync(counts, S->d_counts, 2 * (size_t)S->max_slots * sizeof(unsigned int),
+                                cudaMemcpyDeviceToHost, S->stream));
+        TG_STRY(cudaMemcpyAsync(slot_points, S->d_slot_points, 2 * (size_t)S->max_slots * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, S->stream));
+        TG_STRY(cudaMemcpyAsync(n_fin_p, S->d_n_finished, sizeof(unsigned int), cudaMemcpyDeviceToHost, S->stream));
+        TG_STRY(cudaMemcpyAsync(steps_p, S->d_steps, sizeof(unsigned long long), cudaMemcpyDeviceToHost, S->stream));
         TG_STRY(cudaStreamSynchronize(S->stream));
+        const unsigned int n_fin = *n_fin_p;
+        const unsigned long long steps = *steps_p;
         S->steps_total = steps;
         S->epochs += 1;
         // result buffers large enough for this epoch's finished streamlines,

@@ -69,21 +69,19 @@ def prepare(field, seeds, domain=None, algorithm=None, *, save_at: float = 1.0,
     if not isinstance(batch_size, (int, np.integer)) or batch_size <= 0:
         raise ValueError("batch_size must be a positive integer.")
 
+    # The default domain (nonzero voxels of an image field) is built only when
+    # no domain is given; the reference builds it eagerly (__init__.py:445-466),
+    # which costs a pass over the whole field per call.
     if nifti.is_image(field):
         if field.ndim != 4:
             raise ValueError("The tracking image must be four-dimensional.")
         tracking_field = field_module.Image(field)
-        domain_image = nifti.Nifti1Image(np.any(tracking_field.values != 0, axis=-1).astype(np.uint8),
-                                         field.affine)
+        image_affine = field.affine
         local_model = local.from_shape(field.shape)
     elif isinstance(field, field_module.BaseField):
         tracking_field = field
         local_model = local.from_shape((field.n_parameters,)) if algorithm is None else None
-        if isinstance(field, field_module.Image):
-            affine = np.linalg.inv(field.inverse_affine)
-            domain_image = nifti.Nifti1Image(np.any(field.values != 0, axis=-1).astype(np.uint8), affine)
-        else:
-            domain_image = None
+        image_affine = np.linalg.inv(field.inverse_affine) if isinstance(field, field_module.Image) else None
     else:
         raise TypeError("field must be a Nifti1Image or a BaseField instance.")
 
@@ -117,8 +115,10 @@ def prepare(field, seeds, domain=None, algorithm=None, *, save_at: float = 1.0,
         tracking_domain = domain_module.Image(domain)
     elif domain is not None:
         tracking_domain = domain
-    elif domain_image is not None:
-        tracking_domain = domain_module.Image(domain_image)
+    elif image_affine is not None:
+        values = tracking_field.values
+        tracking_domain = domain_module.Image(
+            nifti.Nifti1Image(np.any(values != 0, axis=-1).astype(np.uint8), image_affine))
     else:
         raise ValueError(
             "A domain is required when the field is not an image field and "
