@@ -47,6 +47,7 @@ import subprocess
 import sys
 import threading
 import time
+import types
 from pathlib import Path
 
 import numpy as np
@@ -751,7 +752,8 @@ def run_product(args):
             for k in range(args.steps):
                 st = {}
                 if kind == "tod":
-                    tracking.tod(algorithm, domain, field, fod, n_seeds, runtime=runtime, stats=st)
+                    grid = types.SimpleNamespace(shape=tuple(shape), affine=np.asarray(fod.affine), header=None)
+                    tracking.tod(algorithm, domain, field, grid, n_seeds, runtime=runtime, stats=st)
                 else:
                     tracking.connectome(algorithm, domain, field, n_seeds, runtime=runtime, stats=st)
                 e2e_steps += st["steps"]

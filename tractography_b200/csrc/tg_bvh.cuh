@@ -221,24 +221,27 @@ __device__ __forceinline__ bool mesh_contains(const MeshDev& m, float x, float y
 }
 
 // Any hit among the leaves of one cell's list (count, then leaf node
-// indices), with max_t = 1 as in the walk's any-hit mode.  The boxes of four
-// leaves are fetched before they are tested.
+// indices), with max_t = 1 as in the walk's any-hit mode.  The boxes of
+// kLeafBatch leaves are fetched before they are tested (more in flight
+// costs registers that the tracking kernels do not have).
+constexpr int kLeafBatch = 2;
+
 __device__ __forceinline__ bool mesh_leaves_hit(const MeshDev& m, const Segment& g, const uint4* list)
 {
     const uint32_t* ids = reinterpret_cast<const uint32_t*>(list);
     const uint32_t count = __ldg(ids);
 #pragma unroll 1
-    for (uint32_t k = 1; k <= count; k += 4) {
-        float4 lo[4], hi[4];
+    for (uint32_t k = 1; k <= count; k += kLeafBatch) {
+        float4 lo[kLeafBatch], hi[kLeafBatch];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kLeafBatch; ++q) {
             // ids past the count are the list's zero padding (node 0, not tested)
             const uint32_t leaf = __ldg(ids + k + q);
             lo[q] = __ldg(m.nodes + 2 * (size_t)leaf);
             hi[q] = __ldg(m.nodes + 2 * (size_t)leaf + 1);
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kLeafBatch; ++q) {
             if (k + (uint32_t)q > count || !box_hit(g, lo[q], hi[q], 1.0f)) continue;
             const int code = __float_as_int(hi[q].w);
             const uint32_t first = (uint32_t)code >> 3;

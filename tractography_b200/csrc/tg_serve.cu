@@ -175,7 +175,7 @@ __device__ __forceinline__ bool s_emit(const ServePool& P, uint32_t avail, int32
 }
 
 template <int MODEL, int LMAX, int ALGO, int DOM>
-__global__ void __launch_bounds__(128, 5) serve_kernel(const ServeParams sp)
+__global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>())) serve_kernel(const ServeParams sp)
 {
     constexpr int CPAD = ModelShape<MODEL, LMAX>::CPAD;
     float c[CPAD];

@@ -15,6 +15,16 @@ struct ModelShape {
     static constexpr int CPAD = (CP + 3) / 4 * 4;
 };
 
+// Resident blocks of 128 lanes per SM that the persistent kernels are
+// compiled for: 5 (at most 102 registers), except the closed-surface
+// variants of the larger SH bands, whose coefficients plus surface-test
+// state do not fit 102 registers without spilling; those get 4 (128).
+template <int MODEL, int LMAX, int DOM>
+constexpr int persistent_min_blocks()
+{
+    return (DOM == kDomainMesh && MODEL != kModelDTI && LMAX >= 6) ? 4 : 5;
+}
+
 struct Lane {
     float px, py, pz;
     float ox, oy, oz;

@@ -93,7 +93,8 @@ __device__ __forceinline__ bool emit_point(const PersistentParams& pp, int32_t& 
 }
 
 template <int MODEL, int LMAX, int ALGO, int DOM>
-__global__ void __launch_bounds__(128, 5) track_persistent_kernel(const PersistentParams pp)
+__global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>())) track_persistent_kernel(
+    const PersistentParams pp)
 {
     constexpr int CPAD = ModelShape<MODEL, LMAX>::CPAD;
     const TrackParams& p = pp.t;
