@@ -86,6 +86,8 @@ def parse_args():
     p.add_argument("--duration", type=float, default=6.0, help="serving: seconds of arrivals per rate")
     p.add_argument("--epoch-steps", type=int, default=65536, help="serving: step cap of an epoch")
     p.add_argument("--epoch-ms", type=float, default=6.0, help="serving: device-clock budget of an epoch (ms)")
+    p.add_argument("--burst", action="store_true",
+                   help="serving: submit the mixed workload's jobs at once and compare with one batched run")
     p.add_argument("--jobs", type=int, default=64, help="jobs of the mixed workload")
     p.add_argument("--per-class", action="store_true",
                    help="mixed: also time each code path's jobs alone (persistent and plain)")
@@ -1083,6 +1085,54 @@ def make_request(volumes, rng):
                                maximum_streamline_length=300.0, batch_size=50000)
 
 
+def run_serve_burst(args):
+    """The mixed workload's jobs submitted to the server at once, against one batched run of them."""
+    import torch
+
+    import tractography_b200 as tg
+    from tractography_b200 import _lib
+    from tractography_b200 import jobs as jobs_module
+    from tractography_b200.serve import Server
+
+    torch.cuda.set_device(0)
+    runtime = tg.CudaRuntime(0)
+    jobs = build_mixed_jobs(args.jobs)
+    kms, waves, launches = ctypes.c_float(), ctypes.c_uint32(), ctypes.c_uint32()
+    for _ in range(2):                          # the second run is the one reported
+        work = jobs_module.run_jobs_packed(jobs, runtime).steps
+        _lib.check(runtime.lib.tg_tracker_stats(runtime.tracker(), ctypes.byref(kms), ctypes.byref(waves),
+                                                ctypes.byref(launches)))
+    batched_kernel_ms = float(kms.value)
+    runs = []
+    for _ in range(2):
+        with Server(runtime, hbm_budget_bytes=150e9, pool_points=256 << 20, epoch_steps=args.epoch_steps,
+                    epoch_seconds=args.epoch_ms * 1e-3, max_requests=128) as server:
+            t0 = time.perf_counter()
+            for job in jobs:
+                server.submit(job)
+            done, polls = 0, 0
+            while done < len(jobs):
+                done += len([server.take(rid, points=False) for rid in server.poll()])
+                polls += 1
+                if polls > 200000:
+                    raise RuntimeError("burst did not finish")
+            wall = time.perf_counter() - t0
+            st = server.stats()
+        runs.append({"wall_s": wall, "busy_s": st.busy_seconds, "kernel_s": st.kernel_seconds,
+                     "between_s": st.between_seconds, "harvest_s": st.harvest_seconds, "epochs": st.epochs,
+                     "steps": st.steps})
+    r = runs[-1]
+    line = {"metric": METRIC, "value": r["steps"] / r["busy_s"], "unit": UNIT, "n_gpus": 1, "steps": 1,
+            "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator; no dataset)", "workload": "serve-burst",
+            "config": {"workload": "the 64 mixed jobs submitted at once to the server",
+                       "epoch_steps": args.epoch_steps, "epoch_ms": args.epoch_ms},
+            "server": r, "server_kernel_steps_per_s": r["steps"] / r["kernel_s"],
+            "batched_kernel_ms": batched_kernel_ms, "batched_steps": work,
+            "batched_kernel_steps_per_s": work / (batched_kernel_ms / 1e3)}
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args):
     """Config 4: continuous-batching server under Poisson arrivals; p50/p99 latency per rate."""
     import torch
@@ -1090,6 +1140,8 @@ def run_serve(args):
     import tractography_b200 as tg
     from tractography_b200.serve import Server
 
+    if args.burst:
+        return run_serve_burst(args)
     torch.cuda.set_device(0)
     runtime = tg.CudaRuntime(0)
     volumes = setup_serving(runtime)
