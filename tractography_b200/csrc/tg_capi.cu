@@ -1222,7 +1222,13 @@ int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_fiel
     q.nz = out_dims[2];
     q.coefficients = coefficients;
     q.steps = reinterpret_cast<unsigned long long*>(steps);
-    TG_TRY(launch_tod(field->d.model, field->d.lmax, q, as_stream(stream)));
+    // the lanes' seed counter: stream-ordered, freed after the launch
+    cudaStream_t s = as_stream(stream);
+    TG_TRY(cudaMallocAsync(reinterpret_cast<void**>(&q.counter), sizeof(unsigned long long), s));
+    cudaError_t e = cudaMemsetAsync(q.counter, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = launch_tod(field->d.model, field->d.lmax, q, s);
+    cudaFreeAsync(q.counter, s);
+    TG_TRY(e);
     return TG_OK;
 }
 
@@ -1260,7 +1266,12 @@ int tg_connectome(const tg_algorithm* algorithm, const tg_domain* domain, const 
     q.columns = columns;
     q.weights = weights;
     q.steps = reinterpret_cast<unsigned long long*>(steps);
-    TG_TRY(launch_connectome(field->d.model, field->d.lmax, q, as_stream(stream)));
+    cudaStream_t s = as_stream(stream);
+    TG_TRY(cudaMallocAsync(reinterpret_cast<void**>(&q.counter), sizeof(unsigned long long), s));
+    cudaError_t e = cudaMemsetAsync(q.counter, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = launch_connectome(field->d.model, field->d.lmax, q, s);
+    cudaFreeAsync(q.counter, s);
+    TG_TRY(e);
     return TG_OK;
 }
 

@@ -175,6 +175,7 @@ struct TodParams {
     uint32_t nx, ny, nz;
     float* coefficients;           // (nx, ny, nz, 45) float32, accumulated
     unsigned long long* steps;     // nullable: loop iterations that passed the domain and field tests
+    unsigned long long* counter;   // next seed index (zeroed by the launcher)
 };
 cudaError_t launch_tod(int model, int lmax, const TodParams& q, cudaStream_t stream);
 
@@ -195,6 +196,7 @@ struct ConnectomeParams {
     int32_t* columns;
     float* weights;
     unsigned long long* steps;     // nullable: loop iterations that passed the domain and field tests
+    unsigned long long* counter;   // next seed index (zeroed by the launcher)
 };
 cudaError_t launch_connectome(int model, int lmax, const ConnectomeParams& q, cudaStream_t stream);
 

@@ -266,14 +266,14 @@ __device__ __forceinline__ void lane_restore(Lane& s, const LaneCarry& c, uint32
     fill = c.fill;
 }
 
-// Adds the steps of the calling lanes (those still running) to *total, one
-// atomic per warp.
-__device__ __forceinline__ void add_steps(unsigned long long* total, uint32_t steps)
+// Adds the steps of the warp's lanes to *total, one atomic per warp; called
+// by all 32 lanes together.
+__device__ __forceinline__ void add_steps64(unsigned long long* total, unsigned long long steps)
 {
     if (total == nullptr) return;
-    const unsigned mask = __activemask();
-    const uint32_t sum = __reduce_add_sync(mask, steps);
-    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(mask) - 1)) atomicAdd(total, (unsigned long long)sum);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) steps += __shfl_xor_sync(0xffffffffu, steps, o);
+    if ((threadIdx.x & 31u) == 0u) atomicAdd(total, steps);
 }
 
 // Tail compaction rule, evaluated by whole warps: once a lane of the warp
