@@ -114,3 +114,32 @@ def test_server_matches_oracle(runtime):
             assert bits_equal(got.streamlines[k], want[i, : want_len[i], :3])
             k += 1
     assert k == len(got.streamlines)
+
+
+def test_results_spanning_several_segments(runtime):
+    """A request that saves far more points per seed than the server's
+    admission estimate gets its result in several segments (new ones start
+    without copying); the points taken back equal the job run alone."""
+    fod, mask = synthetic.bundle_field((14, 14, 14), lmax=8, seed=2)
+    seeds = synthetic.uniform_seeds(mask, 400, seed=9)
+    model = tg.local.RealSymmetricSphericalHarmonics(45)
+    alg = tg.algorithm.Diffusion(model, step_size=0.2, gamma=1.0, noise_variance=0.1, seed=5)
+    job = jobs_module.prepare(tg.field.Image(fod), seeds, tg.domain.Image(mask), alg, save_at=0.05,
+                              maximum_streamline_length=40.0, batch_size=128)
+    alone = run_alone(job, runtime)
+    assert alone.lengths.mean() > 160          # beyond the admission estimate of 160 points per seed
+    with Server(runtime, hbm_budget_bytes=4e9, epoch_steps=9) as server:
+        rid = server.submit(job)
+        results = {}
+        polls = 0
+        while rid not in results:
+            for r in server.poll():
+                results[r] = server.take(r)
+            polls += 1
+            assert polls < 20000
+        assert server.stats().epochs > 10
+    points, offsets, lengths, _ = results[rid]
+    assert np.array_equal(lengths, alone.lengths)
+    for i in range(len(lengths)):
+        assert bits_equal(points[offsets[i]:offsets[i] + lengths[i]],
+                          alone.points[alone.offsets[i]:alone.offsets[i] + alone.lengths[i]]), i

@@ -80,8 +80,9 @@ struct ServeJob {
     unsigned int* counts;       // [0] streamlines in flight, [1] overflowed
     uint32_t chunks_needed;     // worst case per streamline: ceil(n_steps / 32)
     unsigned long long* finished_points;   // points of streamlines finished this epoch
-    float* result;              // (capacity, 3) harvested points
-    uint64_t* result_offset;    // per seed: first point in `result`
+    float* result;              // current result segment: (capacity, 3) harvested points
+    uint64_t result_first;      // request-wide index of the segment's first point
+    uint64_t* result_offset;    // per seed: request-wide index of its first point
     unsigned long long* cursor; // points harvested so far
 };
 
@@ -397,7 +398,7 @@ __global__ void __launch_bounds__(256) harvest_kernel(const ServeJob* __restrict
             const uint32_t j = base + lane;
             if (j < len) {
                 const float* src = pool + ((size_t)chunk * kChunkPoints + lane) * 3;
-                float* dst = J.result + (off + j) * 3;
+                float* dst = J.result + (off - J.result_first + j) * 3;
                 dst[0] = src[0];
                 dst[1] = src[1];
                 dst[2] = src[2];
@@ -442,6 +443,12 @@ double now_s()
 
 using namespace tg;
 
+struct ResultSegment {
+    float* ptr = nullptr;
+    uint64_t first = 0;         // request-wide index of its first point
+    uint64_t cap = 0;           // points
+};
+
 struct ServeRequest {
     uint64_t id = 0;
     int kind = 0;
@@ -458,8 +465,9 @@ struct ServeRequest {
     uint32_t* d_lengths = nullptr;
     int32_t* d_first = nullptr;
     uint64_t* d_offset = nullptr;
-    float* d_result = nullptr;
-    uint64_t result_cap = 0;    // points
+    // Harvested points live in segments: when an epoch's points do not fit
+    // the current one, a new segment starts at the next point (no copy).
+    std::vector<ResultSegment> segments;
     uint64_t harvested = 0;     // points
     std::deque<std::pair<uint32_t, uint32_t>> queue;   // (first seed, count) not yet taken
     double t_submit = 0.0;
@@ -470,7 +478,7 @@ struct ServeResult {
     uint64_t n_points = 0;
     uint32_t* d_lengths = nullptr;
     uint64_t* d_offset = nullptr;
-    float* d_points = nullptr;
+    std::vector<ResultSegment> segments;
     uint64_t bytes = 0;
     double t_submit = 0.0, t_done = 0.0;
 };
@@ -546,16 +554,18 @@ int sfail_cuda(cudaError_t e, const char* what)
 
 void free_request_buffers(tg_server* S, ServeRequest* r)
 {
-    void* bufs[] = {r->d_seeds, r->d_inside, r->d_rng, r->d_first, r->d_lengths, r->d_offset, r->d_result};
+    void* bufs[] = {r->d_seeds, r->d_inside, r->d_rng, r->d_first, r->d_lengths, r->d_offset};
     for (void* b : bufs)
         if (b) cudaFreeAsync(b, S->stream);
+    for (ResultSegment& g : r->segments)
+        if (g.ptr) cudaFreeAsync(g.ptr, S->stream);
+    r->segments.clear();
     r->d_seeds = nullptr;
     r->d_inside = nullptr;
     r->d_rng = nullptr;
     r->d_first = nullptr;
     r->d_lengths = nullptr;
     r->d_offset = nullptr;
-    r->d_result = nullptr;
 }
 
 int write_slot(tg_server* S, int slot)
@@ -578,13 +588,15 @@ int admit(tg_server* S)
             }
         if (slot < 0 || S->fixed + S->reserved + r->reserve > S->budget) return TG_OK;
         const uint32_t n = r->job.n_seeds;
-        r->result_cap = std::max<uint64_t>(1024, (uint64_t)n * std::min<uint64_t>(r->job.n_steps, S->points_estimate));
+        ResultSegment seg;
+        seg.cap = std::max<uint64_t>(1024, (uint64_t)n * std::min<uint64_t>(r->job.n_steps, S->points_estimate));
         TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_seeds), (size_t)n * 32, S->mempool, S->stream));
         TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_rng), (size_t)r->n_batches * 4, S->mempool, S->stream));
         TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_lengths), (size_t)n * 4, S->mempool, S->stream));
         TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_first), (size_t)n * 4, S->mempool, S->stream));
         TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_offset), (size_t)n * 8, S->mempool, S->stream));
-        TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->d_result), r->result_cap * 12, S->mempool, S->stream));
+        TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&seg.ptr), seg.cap * 12, S->mempool, S->stream));
+        r->segments.assign(1, seg);
         // pageable copies are staged before cudaMemcpyAsync returns
         TG_STRY(cudaMemcpyAsync(r->d_seeds, r->host_seeds, (size_t)n * 32, cudaMemcpyHostToDevice, S->stream));
         TG_STRY(cudaMemcpyAsync(r->d_rng, r->host_rng, (size_t)r->n_batches * 4, cudaMemcpyHostToDevice, S->stream));
@@ -608,7 +620,8 @@ int admit(tg_server* S)
         J.counts = S->d_counts + 2 * slot;
         J.finished_points = S->d_slot_points + 2 * slot;
         J.cursor = S->d_slot_points + 2 * slot + 1;
-        J.result = r->d_result;
+        J.result = seg.ptr;
+        J.result_first = 0;
         J.result_offset = r->d_offset;
         J.chunks_needed = (r->job.n_steps + kChunkPoints - 1) / kChunkPoints;
         int st = write_slot(S, slot);
@@ -666,11 +679,11 @@ void complete(tg_server* S, int slot)
     res.t_done = now_s();
     res.d_lengths = r->d_lengths;
     res.d_offset = r->d_offset;
-    res.d_points = r->d_result;
-    res.bytes = r->result_cap * 12 + (uint64_t)res.n_seeds * 12;
+    res.segments.swap(r->segments);
+    res.bytes = (uint64_t)res.n_seeds * 12;
+    for (const ResultSegment& g : res.segments) res.bytes += g.cap * 12;
     r->d_lengths = nullptr;
     r->d_offset = nullptr;
-    r->d_result = nullptr;
     free_request_buffers(S, r);
     S->reserved -= r->reserve;
     S->reserved += res.bytes;
@@ -712,21 +725,20 @@ int requeue_overflow(tg_server* S, int slot)
     return TG_OK;
 }
 
-// Grow a request's result buffer to hold `need` points (stream-ordered copy).
-int grow_result(tg_server* S, int slot, uint64_t need)
+// Start a new result segment at the request's next point, large enough for
+// `add` more points (at least twice the last segment); nothing is copied.
+int new_result_segment(tg_server* S, int slot, uint64_t add)
 {
     ServeRequest* r = S->slots[slot];
-    uint64_t cap = std::max<uint64_t>(need, 2 * r->result_cap);
-    float* fresh = nullptr;
-    TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&fresh), cap * 12, S->mempool, S->stream));
-    if (r->harvested > 0)
-        TG_STRY(cudaMemcpyAsync(fresh, r->d_result, r->harvested * 12, cudaMemcpyDeviceToDevice, S->stream));
-    TG_STRY(cudaFreeAsync(r->d_result, S->stream));
-    S->reserved += (cap - r->result_cap) * 12;
-    r->reserve += (cap - r->result_cap) * 12;
-    r->d_result = fresh;
-    r->result_cap = cap;
-    S->h_jobs[slot].result = fresh;
+    ResultSegment seg;
+    seg.first = r->harvested;
+    seg.cap = std::max<uint64_t>(add, r->segments.empty() ? 1024 : 2 * r->segments.back().cap);
+    TG_STRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&seg.ptr), seg.cap * 12, S->mempool, S->stream));
+    S->reserved += seg.cap * 12;
+    r->reserve += seg.cap * 12;
+    r->segments.push_back(seg);
+    S->h_jobs[slot].result = seg.ptr;
+    S->h_jobs[slot].result_first = seg.first;
     return write_slot(S, slot);
 }
 
@@ -823,9 +835,11 @@ int tg_server_destroy(tg_server* S)
         }
     for (ServeRequest* r : S->pending) delete r;
     for (auto& kv : S->results) {
-        void* bufs[] = {kv.second.d_points, kv.second.d_lengths, kv.second.d_offset};
+        void* bufs[] = {kv.second.d_lengths, kv.second.d_offset};
         for (void* b : bufs)
             if (b) cudaFreeAsync(b, S->stream);
+        for (const ResultSegment& g : kv.second.segments)
+            if (g.ptr) cudaFreeAsync(g.ptr, S->stream);
     }
     if (S->stream) cudaStreamSynchronize(S->stream);
     for (int k = 0; k < kServeKinds; ++k) {
@@ -1044,8 +1058,9 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
             ServeRequest* r = S->slots[slot];
             const uint64_t add = slot_points[2 * slot];
             if (add == 0) continue;
-            if (r->harvested + add > r->result_cap) {
-                st = grow_result(S, (int)slot, r->harvested + add);
+            const ResultSegment& cur = r->segments.back();
+            if (r->harvested + add > cur.first + cur.cap) {
+                st = new_result_segment(S, (int)slot, add);
                 if (st != TG_OK) return st;
             }
             r->harvested += add;
@@ -1137,11 +1152,18 @@ int tg_server_take(tg_server* S, uint64_t request_id, uint32_t* lengths, uint64_
         TG_STRY(cudaMemcpyAsync(lengths, res.d_lengths, (size_t)res.n_seeds * 4, cudaMemcpyDeviceToHost, S->stream));
     if (res.n_seeds > 0 && offsets)
         TG_STRY(cudaMemcpyAsync(offsets, res.d_offset, (size_t)res.n_seeds * 8, cudaMemcpyDeviceToHost, S->stream));
-    if (res.n_points > 0 && points)
-        TG_STRY(cudaMemcpyAsync(points, res.d_points, res.n_points * 12, cudaMemcpyDeviceToHost, S->stream));
-    void* bufs[] = {res.d_points, res.d_lengths, res.d_offset};
+    for (size_t k = 0; k < res.segments.size(); ++k) {
+        const ResultSegment& g = res.segments[k];
+        const uint64_t end = k + 1 < res.segments.size() ? res.segments[k + 1].first : res.n_points;
+        if (points && end > g.first)
+            TG_STRY(cudaMemcpyAsync(points + g.first * 3, g.ptr, (end - g.first) * 12, cudaMemcpyDeviceToHost,
+                                    S->stream));
+    }
+    void* bufs[] = {res.d_lengths, res.d_offset};
     for (void* b : bufs)
         if (b) TG_STRY(cudaFreeAsync(b, S->stream));
+    for (const ResultSegment& g : res.segments)
+        if (g.ptr) TG_STRY(cudaFreeAsync(g.ptr, S->stream));
     TG_STRY(cudaStreamSynchronize(S->stream));
     S->reserved -= std::min(S->reserved, res.bytes);
     S->results.erase(it);
