@@ -260,6 +260,10 @@ int tg_server_take(tg_server* server, uint64_t request_id, uint32_t* lengths, ui
                    float* points);
 int tg_server_stats(const tg_server* server, uint64_t* steps, uint64_t* epochs, double* busy_seconds,
                     uint64_t* reserved_bytes);
+/* Map `bytes` of device memory into the server's memory pool now (they stay
+ * reserved for request buffers and results, up to the budget), so that
+ * admissions and growing results do not map memory between epochs. */
+int tg_server_reserve(tg_server* server, uint64_t bytes);
 /* Device-clock budget of an epoch in seconds (0, the default: epoch_steps
  * alone ends an epoch).  With a budget, every code path's lanes stop at the
  * same deadline, whatever their step cost; results do not change. */

@@ -59,6 +59,7 @@ EXPORTS = (
     "tg_server_take",
     "tg_server_stats",
     "tg_server_set_epoch_time",
+    "tg_server_reserve",
     "tg_server_timing",
     "tg_seeds_from_fod",
     "tg_domain_contains",
@@ -164,6 +165,7 @@ def load() -> ctypes.CDLL:
                                   ctypes.c_int),
         "tg_server_take": ([P, U64, P, P, P], ctypes.c_int),
         "tg_server_set_epoch_time": ([P, ctypes.c_double], ctypes.c_int),
+        "tg_server_reserve": ([P, U64], ctypes.c_int),
         "tg_server_timing": ([P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                               ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
         "tg_server_stats": ([P, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(ctypes.c_double),

@@ -945,18 +945,17 @@ int tg_server_poll(tg_server* S, uint64_t* finished_ids, uint32_t capacity, uint
     if (any) {
         const double t0 = now_s();
         int grid[kServeKinds] = {};
-        double want_total = 0.0;
-        for (int k = 0; k < kServeKinds; ++k) want_total += (double)n_new[k] + S->carry_n[k];
         for (int k = 0; k < kServeKinds; ++k) {
             if (n_new[k] == 0 && S->carry_n[k] == 0) continue;
-            // every kind gets the lanes its carried streamlines need; the rest
-            // of the GPU is shared in proportion to queued work
+            // every kind is launched with as many blocks as its work fills,
+            // up to a full GPU, on its own stream: the block scheduler gives
+            // SMs freed by a kind whose queue drained to the others (a fixed
+            // split would leave them idle until the deadline).  At least one
+            // lane per carried streamline (it resumes in the lane's first fetch).
             const int full = S->sms * kind_blocks(S, k);
             const int need = (int)((S->carry_n[k] + 127) / 128);
-            const int share = (int)std::ceil(full * (((double)n_new[k] + S->carry_n[k]) / want_total));
             const int work = (int)std::min<uint64_t>((uint64_t)full, (n_new[k] + S->carry_n[k] + 127) / 128);
-            grid[k] = std::max(need, std::min(work, std::max(share, S->sms / 4)));
-            grid[k] = std::max(1, std::min(grid[k], full));
+            grid[k] = std::max(1, std::max(need, work));
             st = ensure_carry(S, k, (size_t)full * 128);
             if (st != TG_OK) return st;
             if (S->kstream[k] == nullptr) {
@@ -1168,6 +1167,20 @@ int tg_server_take(tg_server* S, uint64_t request_id, uint32_t* lengths, uint64_
     S->reserved -= std::min(S->reserved, res.bytes);
     S->results.erase(it);
     return admit(S);
+}
+
+int tg_server_reserve(tg_server* S, uint64_t bytes)
+{
+    if (S == nullptr) return sfail(TG_ERR_INVALID_ARGUMENT, "server is null");
+    if (bytes == 0) return TG_OK;
+    // allocate and free once: the pool keeps the memory (its release
+    // threshold is the budget), so later request buffers are carved from it
+    // instead of mapping new memory while requests wait
+    void* p = nullptr;
+    TG_STRY(cudaMallocFromPoolAsync(&p, bytes, S->mempool, S->stream));
+    TG_STRY(cudaFreeAsync(p, S->stream));
+    TG_STRY(cudaStreamSynchronize(S->stream));
+    return TG_OK;
 }
 
 int tg_server_set_epoch_time(tg_server* S, double seconds)

@@ -52,10 +52,15 @@ class Server:
         max_requests: admitted requests at a time.
         epoch_seconds: device-clock budget of an epoch (0: epoch_steps
             alone ends it); every code path stops at the same deadline.
+        reserve_bytes: device memory mapped into the server's pool at
+            creation for request buffers and results (default: the budget
+            less the point pool, at most 90 % of the free memory); 0 maps
+            on demand, which costs time between epochs.
     """
 
     def __init__(self, runtime=None, *, hbm_budget_bytes: float = 150e9, pool_points: int = 0,
-                 epoch_steps: int = 1024, max_requests: int = 256, epoch_seconds: float = 0.0):
+                 epoch_steps: int = 1024, max_requests: int = 256, epoch_seconds: float = 0.0,
+                 reserve_bytes: int | None = None):
         from .runtime import default_runtime
 
         self.runtime = runtime or default_runtime()
@@ -66,6 +71,14 @@ class Server:
                                                  int(max_requests), ctypes.byref(self._handle)))
             if epoch_seconds:
                 _lib.check(self.lib.tg_server_set_epoch_time(self._handle, float(epoch_seconds)))
+            if reserve_bytes is None:
+                import torch
+
+                free, _ = torch.cuda.mem_get_info(self.runtime.device)
+                pool = (pool_points or (32 << 20)) * 12
+                reserve_bytes = int(max(0.0, min(hbm_budget_bytes - pool, 0.9 * free - pool)))
+            if reserve_bytes > 0:
+                _lib.check(self.lib.tg_server_reserve(self._handle, int(reserve_bytes)))
         self._jobs = {}
         self._arrays = {}
         self._ids = (ctypes.c_uint64 * 1024)()
