@@ -40,12 +40,17 @@ def test_tod_matches_oracle(runtime, kind):
     make = (lambda: tg.algorithm.Transport(model, step_size=0.1, gamma=1.0)) if kind == "transport" else \
         (lambda: tg.algorithm.Diffusion(model, step_size=0.1, gamma=1.0, noise_variance=0.05, seed=3))
     alg, twin = make(), make()
+    stats = {}
     got = tg.tracking.tod(alg, domain, field, tg.Nifti1Image(np.zeros((12, 12, 3)), np.eye(4)), 3000,
-                          maximum_streamline_length=8.0, runtime=runtime)
+                          maximum_streamline_length=8.0, runtime=runtime, stats=stats)
     raw = oracle_case(twin, domain, field, rng_seed=twin.get_rng_seed()).tod(
         domain.boundary_arrays(), 3000, 80, (12, 12, 3), np.eye(4))
     _compare(np.asarray(got.dataobj), tg.utils.normalize_odf(raw))
     assert np.count_nonzero(np.asarray(got.dataobj)[..., 0]) > 10
+    # every accepted step inside the output grid added Y00 = 1 / (2 sqrt(pi)) to raw[..., 0]
+    assert stats["steps"] <= 3000 * 80
+    inside = float(raw[..., 0].sum(dtype=np.float64)) * 2.0 * np.sqrt(np.pi)   # float32 sums: to 1e-3
+    assert stats["steps"] >= 0.999 * inside > 0
 
 
 def test_tg_tod_reference_cases(runtime):
