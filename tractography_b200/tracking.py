@@ -194,7 +194,7 @@ def tod(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, image, n
     if not np.isfinite(step_size) or step_size <= 0:
         raise ValueError("algorithm.step_size must be finite and positive.")
     n_steps = int(np.floor(maximum_streamline_length / step_size))
-    raw = np.zeros(output_shape + (45,), dtype=np.float32)
+    header = getattr(image, "header", None)
     if n_seeds > 0 and n_steps > 0:
         from .runtime import default_runtime
 
@@ -207,8 +207,9 @@ def tod(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, image, n
             a = to_struct(algorithm, algorithm.get_rng_seed(),
                           algorithm.philox_key() if algorithm.rng_mode() == _lib.RNG_PHILOX else 0, 0)
             dv, df, dc = runtime.to_device(v4), runtime.to_device(f4), runtime.to_device(cumulative)
-            coefficients = torch.zeros(output_shape + (45,), dtype=torch.float32, device=runtime.device)
-            steps = torch.zeros((1,), dtype=torch.int64, device=runtime.device)
+            with torch.cuda.stream(runtime.stream):    # zeroed on the stream the kernel runs on
+                coefficients = torch.zeros(output_shape + (45,), dtype=torch.float32, device=runtime.device)
+                steps = torch.zeros((1,), dtype=torch.int64, device=runtime.device)
             dims = np.asarray(output_shape, dtype=np.uint32)
             _lib.check(runtime.lib.tg_tod(
                 ctypes.byref(a), d_handle, f_handle, ctypes.c_void_p(dv.data_ptr()), len(v4),
@@ -216,10 +217,19 @@ def tod(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, image, n
                 dims.ctypes.data_as(ctypes.c_void_p), inverse_affine.ctypes.data_as(ctypes.c_void_p),
                 ctypes.c_void_p(coefficients.data_ptr()), ctypes.c_void_p(steps.data_ptr()),
                 ctypes.c_void_p(runtime.stream_handle)))
-            raw = coefficients.cpu().numpy()
-            if stats is not None:
-                stats["steps"] = int(steps.item())
-    header = getattr(image, "header", None)
+            # normalize_odf on the device, in its float64 operations
+            # (c / sqrt(4 pi) / c0, rounded to float32; zero where c0 == 0),
+            # then one copy of the result to page-locked host memory
+            out = runtime.pinned(output_shape + (45,), np.float32)
+            with torch.cuda.stream(runtime.stream):
+                c0 = coefficients[..., :1]
+                normalized = torch.where(c0 != 0, (coefficients.double() / np.sqrt(4 * np.pi) / c0.double()).float(),
+                                         torch.zeros((), dtype=torch.float32, device=coefficients.device))
+                torch.from_numpy(out).copy_(normalized)
+                if stats is not None:
+                    stats["steps"] = int(steps.item())
+            return Nifti1Image(out, affine, header)
+    raw = np.zeros(output_shape + (45,), dtype=np.float32)
     return Nifti1Image(normalize_odf(raw).astype(np.float32), affine, header)
 
 
@@ -271,16 +281,18 @@ def connectome(algorithm: BaseAlgorithm, domain: BaseDomain, field: BaseField, n
         rows = runtime.empty((9 * int(n_seeds),), torch.int32)
         cols = runtime.empty((9 * int(n_seeds),), torch.int32)
         weights = runtime.empty((9 * int(n_seeds),), torch.float32)
-        steps = torch.zeros((1,), dtype=torch.int64, device=runtime.device)
+        with torch.cuda.stream(runtime.stream):        # zeroed on the stream the kernel runs on
+            steps = torch.zeros((1,), dtype=torch.int64, device=runtime.device)
         _lib.check(runtime.lib.tg_connectome(
             ctypes.byref(a), d_handle, f_handle, b_handle, ctypes.c_void_p(dv.data_ptr()), len(v4),
             ctypes.c_void_p(df.data_ptr()), ctypes.c_void_p(dc.data_ptr()), len(f4), int(n_seeds), n_steps,
             float(minimum_streamline_length), ctypes.c_void_p(rows.data_ptr()), ctypes.c_void_p(cols.data_ptr()),
             ctypes.c_void_p(weights.data_ptr()), ctypes.c_void_p(steps.data_ptr()),
             ctypes.c_void_p(runtime.stream_handle)))
-        rows, cols, weights = rows.cpu().numpy(), cols.cpu().numpy(), weights.cpu().numpy()
-        if stats is not None:
-            stats["steps"] = int(steps.item())
+        with torch.cuda.stream(runtime.stream):
+            rows, cols, weights = rows.cpu().numpy(), cols.cpu().numpy(), weights.cpu().numpy()
+            if stats is not None:
+                stats["steps"] = int(steps.item())
     return contributions_to_matrix(rows, cols, weights, n_vertices)
 
 
