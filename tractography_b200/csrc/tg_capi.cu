@@ -180,15 +180,6 @@ int make_track_params(const tg_algorithm* a, const tg_domain* d, const tg_field*
     p.algo = algo_params(a);
     p.save_at = save_at;
     p.n_steps = n_steps;
-    // A step of at least 1/50 voxel (largest row of the field's inverse
-    // affine) changes voxel often enough that fetching the next voxel into L2
-    // one step ahead pays for the extra index arithmetic.
-    double row_max = 0.0;
-    for (int r = 0; r < 3; ++r) {
-        const float* m = f->d.inv_affine + 4 * r;
-        row_max = std::max(row_max, std::sqrt((double)m[0] * m[0] + (double)m[1] * m[1] + (double)m[2] * m[2]));
-    }
-    p.prefetch = d->d.kind == kDomainImage && (double)p.algo.step_size * row_max >= 0.02 ? 1 : 0;
     *out = p;
     return TG_OK;
 }

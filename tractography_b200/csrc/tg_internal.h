@@ -62,7 +62,6 @@ struct TrackParams {
     const float* field;
     uint32_t cpad;
     int same_grid;           // domain and field inverse affines/dims identical
-    int prefetch;            // steps cross voxels often: prefetch the next voxel into L2
     int algorithm;           // kTransport or kDiffusion
     AlgoParams algo;
     float save_at;

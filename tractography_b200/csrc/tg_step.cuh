@@ -165,25 +165,6 @@ __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (
     s.px = fmaf(step, s.ox, s.px);
     s.py = fmaf(step, s.oy, s.py);
     s.pz = fmaf(step, s.oz, s.pz);
-    if (DOM == kDomainImage && p.prefetch) {
-        // Bring the voxel the iteration after next will most likely gather
-        // into L2 now, a full step ahead: the point one more step along the
-        // current orientation (which turns slowly).  A hint only -- no
-        // result depends on it, a wrong guess wastes a prefetch.  A padded
-        // voxel spans at most two 128-byte lines, so its first and last
-        // bytes cover it.
-        const float gx = fmaf(step, s.ox, s.px), gy = fmaf(step, s.oy, s.py), gz = fmaf(step, s.oz, s.pz);
-        const float fx = rintf(dot4(p.fgrid.row0, gx, gy, gz, 1.0f));
-        const float fy = rintf(dot4(p.fgrid.row1, gx, gy, gz, 1.0f));
-        const float fz = rintf(dot4(p.fgrid.row2, gx, gy, gz, 1.0f));
-        if ((fx != s.fvx || fy != s.fvy || fz != s.fvz) && fx >= 0.0f && fx < (float)p.fgrid.nx && fy >= 0.0f &&
-            fy < (float)p.fgrid.ny && fz >= 0.0f && fz < (float)p.fgrid.nz) {
-            const int64_t fv = ((int64_t)(int32_t)fx * p.fgrid.ny + (int32_t)fy) * p.fgrid.nz + (int32_t)fz;
-            const float* v = p.field + fv * CPAD;
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(v));
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(v + CPAD - 1));
-        }
-    }
     s.time = s.time + step;
     if (s.time >= p.save_at) {
         s.time = s.time - p.save_at;
