@@ -267,30 +267,108 @@ __device__ __forceinline__ bool mesh_leaves_hit(const MeshDev& m, const Segment&
 //     reaches a leaf exactly when the leaf's own box test passes, and the
 //     any-hit over the list equals the walk's;
 //   - otherwise the any-hit walk from the root.
-__device__ __forceinline__ bool mesh_segment_blocked(const MeshDev& m, float sx, float sy, float sz, float ex,
-                                                     float ey, float ez)
+// Which route decides a segment: 0 the distance grid (nothing can be hit),
+// 1 the start cell's leaf list (its offset in `list`), 2 the walk.
+__device__ __forceinline__ int mesh_route(const MeshDev& m, float sx, float sy, float sz, float ex, float ey,
+                                          float ez, uint32_t& list)
 {
     const float usx = (sx - m.ox) * m.inv_cell, usy = (sy - m.oy) * m.inv_cell, usz = (sz - m.oz) * m.inv_cell;
     const float uex = (ex - m.ox) * m.inv_cell, uey = (ey - m.oy) * m.inv_cell, uez = (ez - m.oz) * m.inv_cell;
     const float ax = floorf(usx), ay = floorf(usy), az = floorf(usz);
     const float bx = floorf(uex), by = floorf(uey), bz = floorf(uez);
-    const Segment g = make_segment(sx, sy, sz, ex, ey, ez);
     if (ax >= 0.0f && ax < m.gx && ay >= 0.0f && ay < m.gy && az >= 0.0f && az < m.gz && bx >= 0.0f &&
         bx < m.gx && by >= 0.0f && by < m.gy && bz >= 0.0f && bz < m.gz) {
         const size_t cell = ((size_t)ax * (size_t)m.gy + (size_t)ay) * (size_t)m.gz + (size_t)az;
         const uint32_t word = __ldg(m.cells + cell);
         const float reach = (float)(word & 255u);
         const float cheb = fmaxf(fmaxf(fabsf(bx - ax), fabsf(by - ay)), fabsf(bz - az));
-        if (cheb < reach) return false;
-        const uint32_t list = word >> 8;
+        if (cheb < reach) return 0;
+        list = word >> 8;
         const float lo = -0.49f, hi = 1.49f;
         if (list != kNoLeafList && uex - ax >= lo && uex - ax <= hi && uey - ay >= lo && uey - ay <= hi &&
             uez - az >= lo && uez - az <= hi)
-            return mesh_leaves_hit(m, g, m.lists + list);
+            return 1;
     }
+    return 2;
+}
+
+__device__ __forceinline__ bool mesh_segment_blocked(const MeshDev& m, float sx, float sy, float sz, float ex,
+                                                     float ey, float ez)
+{
+    uint32_t list = 0;
+    const int route = mesh_route(m, sx, sy, sz, ex, ey, ez, list);
+    if (route == 0) return false;
+    const Segment g = make_segment(sx, sy, sz, ex, ey, ez);
+    if (route == 1) return mesh_leaves_hit(m, g, m.lists + list);
     float t, u, v;
     uint32_t tri;
     return mesh_walk<1>(m, g, t, tri, u, v) != 0u;
+}
+
+// The leaf-list route for a whole warp at once.  Called by all 32 lanes
+// together; lanes with `need` set have a segment g and a leaf list.  The
+// warp's (lane, leaf) pairs are dealt to its lanes, one pair per lane per
+// round -- the owner's segment comes by shuffle -- so a few lanes near the
+// surface no longer run their lists one after the other while the rest of
+// the warp waits.  Any-hit is independent of the order of the tests, so
+// each lane's answer is the one mesh_leaves_hit gives.
+__device__ __forceinline__ bool warp_leaves_hit(const MeshDev& m, bool need, const Segment& g, uint32_t list)
+{
+    constexpr unsigned kFull = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t count = need ? __ldg(reinterpret_cast<const uint32_t*>(m.lists + list)) : 0u;
+    uint32_t incl = count;
+#pragma unroll
+    for (uint32_t o = 1; o < 32u; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t flags = (g.px ? 1u : 0u) | (g.py ? 2u : 0u) | (g.pz ? 4u : 0u);
+    unsigned hits = 0u;
+    for (uint32_t base = 0; base < total; base += 32u) {
+        const uint32_t w = base + lane;
+        // owner: the first lane whose inclusive count exceeds w
+        uint32_t owner = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0u; step >>= 1) {
+            const uint32_t v = __shfl_sync(kFull, incl, owner + step - 1u);
+            if (v <= w) owner += step;
+        }
+        const uint32_t first = __shfl_sync(kFull, incl, owner) - __shfl_sync(kFull, count, owner);
+        Segment o;
+        o.sx = __shfl_sync(kFull, g.sx, owner);
+        o.sy = __shfl_sync(kFull, g.sy, owner);
+        o.sz = __shfl_sync(kFull, g.sz, owner);
+        o.dx = __shfl_sync(kFull, g.dx, owner);
+        o.dy = __shfl_sync(kFull, g.dy, owner);
+        o.dz = __shfl_sync(kFull, g.dz, owner);
+        o.ix = __shfl_sync(kFull, g.ix, owner);
+        o.iy = __shfl_sync(kFull, g.iy, owner);
+        o.iz = __shfl_sync(kFull, g.iz, owner);
+        const uint32_t of = __shfl_sync(kFull, flags, owner);
+        o.px = (of & 1u) != 0u;
+        o.py = (of & 2u) != 0u;
+        o.pz = (of & 4u) != 0u;
+        const uint32_t olist = __shfl_sync(kFull, list, owner);
+        bool h = false;
+        if (w < total) {
+            const uint32_t leaf = __ldg(reinterpret_cast<const uint32_t*>(m.lists + olist) + 1u + (w - first));
+            const float4 lo = __ldg(m.nodes + 2 * (size_t)leaf);
+            const float4 hi = __ldg(m.nodes + 2 * (size_t)leaf + 1);
+            if (box_hit(o, lo, hi, 1.0f)) {
+                const int code = __float_as_int(hi.w);
+                const uint32_t tfirst = (uint32_t)code >> 3;
+                const uint32_t tn = (uint32_t)code & 7u;
+                for (uint32_t j = 0; j < tn && !h; ++j) {
+                    float tt, uu, vv;
+                    h = triangle_hit(o, m.tris + 3 * (size_t)(tfirst + j), 1.0f, tt, uu, vv);
+                }
+            }
+        }
+        hits |= __reduce_or_sync(kFull, h ? (1u << owner) : 0u);
+    }
+    return need && ((hits >> lane) & 1u) != 0u;
 }
 
 }  // namespace tg

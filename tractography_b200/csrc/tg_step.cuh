@@ -18,11 +18,12 @@ struct ModelShape {
 // Resident blocks of 128 lanes per SM that the persistent kernels are
 // compiled for: 5 (at most 102 registers), except the closed-surface
 // variants of the larger SH bands, whose coefficients plus surface-test
-// state do not fit 102 registers without spilling; those get 4 (128).
+// state do not fit 102 registers without spilling (4 blocks, 128), and the
+// closed-surface tensor variant, whose few coefficients leave room for 6 (85).
 template <int MODEL, int LMAX, int DOM>
 constexpr int persistent_min_blocks()
 {
-    return (DOM == kDomainMesh && MODEL != kModelDTI && LMAX >= 6) ? 4 : 5;
+    return DOM == kDomainMesh ? (MODEL == kModelDTI ? 6 : (LMAX >= 6 ? 4 : 5)) : 5;
 }
 
 struct Lane {
@@ -56,15 +57,18 @@ struct Lane {
 // The domain test and the field gather of one iteration (tracking.py:123-
 // 133): false when the streamline stops; otherwise c holds the coefficients
 // of the nearest field voxel.
+// `surface` (closed surface, after the first step): the segment test's
+// answer when the caller computed it for the whole warp (0 clear, 1
+// blocked), -1 to compute it here.
 template <int MODEL, int LMAX, int CPAD, int DOM>
-__device__ __forceinline__ bool locate(const TrackParams& p, Lane& s, float (&c)[CPAD])
+__device__ __forceinline__ bool locate(const TrackParams& p, Lane& s, float (&c)[CPAD], int surface = -1)
 {
     float ax, ay, az;
     if constexpr (DOM == kDomainMesh) {
         if (s.steps == 0u) {
             const bool inside = s.seed_state == 0u ? mesh_contains(p.mesh, s.px, s.py, s.pz) : s.seed_state == 1u;
             if (!inside) return false;
-        } else if (mesh_segment_blocked(p.mesh, s.lx, s.ly, s.lz, s.px, s.py, s.pz)) {
+        } else if (surface >= 0 ? surface != 0 : mesh_segment_blocked(p.mesh, s.lx, s.ly, s.lz, s.px, s.py, s.pz)) {
             return false;
         }
         s.lx = s.px;
@@ -155,9 +159,9 @@ __device__ __forceinline__ bool locate(const TrackParams& p, Lane& s, float (&c)
 
 template <int MODEL, int LMAX, int ALGO, int CPAD, int DOM = kDomainImage>
 __device__ __forceinline__ int track_step(const TrackParams& p, Lane& s, float (&c)[CPAD],
-                                          float& qx, float& qy, float& qz)
+                                          float& qx, float& qy, float& qz, int surface = -1)
 {
-    if (!locate<MODEL, LMAX, CPAD, DOM>(p, s, c)) return 0;
+    if (!locate<MODEL, LMAX, CPAD, DOM>(p, s, c, surface)) return 0;
     update_orientation<MODEL, LMAX, ALGO>(p.algo, c, s.ox, s.oy, s.oz, s.rng);
     s.steps += 1u;
 

@@ -147,12 +147,31 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
             if (live) lane_save(pp.carry_out + atomicAdd(pp.carry_out_count, 1u), s, item, chunk, fill);
             break;
         }
+        // Closed surface: the segment tests of this iteration, done here while
+        // the warp is together, so that leaf-list tests are shared out over
+        // all its lanes (warp_leaves_hit); same answers as a test per lane.
+        int surface = -1;
+        if constexpr (DOM == kDomainMesh) {
+            const bool testing = live && s.n < p.n_steps && s.steps > 0u;
+            uint32_t list = 0;
+            int route = 0;
+            Segment g;
+            g.sx = g.sy = g.sz = g.dx = g.dy = g.dz = g.ix = g.iy = g.iz = 0.0f;
+            g.px = g.py = g.pz = false;
+            if (testing) {
+                route = mesh_route(p.mesh, s.lx, s.ly, s.lz, s.px, s.py, s.pz, list);
+                if (route == 1) g = make_segment(s.lx, s.ly, s.lz, s.px, s.py, s.pz);
+            }
+            bool hit = false;
+            if (__any_sync(0xffffffffu, route == 1)) hit = warp_leaves_hit(p.mesh, route == 1, g, list);
+            if (testing) surface = route == 0 ? 0 : (route == 1 ? (hit ? 1 : 0) : -1);
+        }
         if (!live) continue;
         bool done = s.n >= p.n_steps;
         bool overflow = false;
         if (!done) {
             float qx, qy, qz;
-            const int r = track_step<MODEL, LMAX, ALGO, CPAD, DOM>(p, s, c, qx, qy, qz);
+            const int r = track_step<MODEL, LMAX, ALGO, CPAD, DOM>(p, s, c, qx, qy, qz, surface);
             if (r == 0) {
                 done = true;
             } else if (r == 2) {
