@@ -122,9 +122,9 @@ def fp32_peak_tflops():
     return props.multi_processor_count * 128 * 2 * clock_khz * 1e3 / 1e12
 
 
-def traffic_per_step():
+def traffic_per_step(profile="track_persistent_config1.md"):
     """DRAM bytes per accepted step of the tracking kernel from the committed ncu summary."""
-    path = ROOT / "profiles" / "track_persistent_config1.md"
+    path = ROOT / "profiles" / profile
     if not path.exists():
         return None
     for line in path.read_text().splitlines():
@@ -1025,6 +1025,7 @@ def run_config2(args):
             e2e_ms = ev0.elapsed_time(ev1)
     peak, peak_kind = measured_peaks()
     kernel_sps = dev_steps / (kernel_ms / 1e3)
+    c2_tps = traffic_per_step("track_persistent_config2.md")
     info = mesh.info(runtime)
     line = {
         "metric": METRIC, "value": dev_steps / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
@@ -1039,7 +1040,10 @@ def run_config2(args):
                 "d2h_bytes_per_step": int(d2h / args.steps)},
         "gpu_launches": n_launch,
         "roofline": {"bound": "hbm", "achieved": kernel_sps * C2_BYTES_PER_STEP / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": kernel_sps * C2_BYTES_PER_STEP / 1e9 / peak, "traffic": None,
+                     "frac": kernel_sps * C2_BYTES_PER_STEP / 1e9 / peak,
+                     "traffic": (c2_tps * dev_steps / args.steps) if c2_tps is not None else None,
+                     "traffic_source": "DRAM bytes per accepted step of the 200k-seed ncu capture "
+                                       "(profiles/track_persistent_config2.md) x the steps of one launch",
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "bytes_per_step": C2_BYTES_PER_STEP,
                      "note": "bytes exclude the BVH nodes and triangles read near the surface",
