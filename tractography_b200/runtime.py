@@ -96,7 +96,7 @@ class CudaRuntime:
         """A page-locked host array (fast device-to-host copies)."""
         torch = _torch()
         t = torch.empty(shape, dtype=_TORCH_DTYPES[np.dtype(dtype)], pin_memory=True)
-        return t.numpy()
+        return t.numpy().view(np.dtype(dtype))      # unsigned types live in same-size signed tensors
 
     def finish(self) -> None:
         """Wait for all work queued on this runtime's stream."""
