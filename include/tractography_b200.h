@@ -367,6 +367,17 @@ int tg_update_orientation(int32_t model, uint32_t n_parameters, const tg_algorit
 int tg_rng_stream(int32_t which, uint32_t s0, uint32_t s1, uint32_t n, uint32_t max, void* out,
                   void* stream);
 
+/* The step limit every tracking entry point applies to a streamline of the
+ * tractogram loop (tracking.py:121-147), which saves a point each time the
+ * binary32 sum time += step_size reaches save_at.  *max_steps receives
+ * n_steps times the most loop iterations that can separate two saved points
+ * (a bound that never ends a streamline the reference would continue).
+ * Returns TG_ERR_INVALID_ARGUMENT when time + step_size == time for some
+ * time below save_at (the reference's loop would then run for ever on a
+ * streamline that stays in the domain) or when the limit exceeds 2^32 - 1;
+ * every tracking entry point rejects the same parameters.  Host only. */
+int tg_step_bound(float step_size, float save_at, uint32_t n_steps, uint64_t* max_steps);
+
 #ifdef __cplusplus
 }
 #endif

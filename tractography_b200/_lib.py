@@ -70,6 +70,7 @@ EXPORTS = (
     "tg_local_evaluate",
     "tg_update_orientation",
     "tg_rng_stream",
+    "tg_step_bound",
 )
 
 
@@ -179,6 +180,7 @@ def load() -> ctypes.CDLL:
         "tg_local_evaluate": ([I32, U32, P, P, U32, P, P], ctypes.c_int),
         "tg_update_orientation": ([I32, U32, AP, P, P, U32, P, P], ctypes.c_int),
         "tg_rng_stream": ([I32, U32, U32, U32, U32, P, P], ctypes.c_int),
+        "tg_step_bound": ([F, F, U32, ctypes.POINTER(U64)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

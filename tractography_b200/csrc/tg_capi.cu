@@ -153,14 +153,86 @@ AlgoParams algo_params(const tg_algorithm* a)
     return p;
 }
 
+}  // namespace
+
+namespace tg {
+
+// The most iterations of tracking.py:121-147 that can separate two saved
+// points, or 0 when some streamline would never save another one.
+//
+// The loop adds step to time in binary32 until time >= save_at.  Rounding
+// is monotonic, so a time that starts higher never falls behind one that
+// starts at 0: the count from time = 0 is the worst case.  In the binade
+// [2^(e-1), 2^e) (spacing u = 2^(e-24)) an iteration whose sum stays in the
+// binade advances time by at least inc = step rounded down to a multiple of
+// u (up to one when the remainder exceeds u/2), and one more iteration
+// leaves the binade.  Where inc is 0 -- step at most half the spacing of
+// the largest float below save_at -- time + step == time for some time and
+// the streamline never ends.  The sum over binades bounds the count.
+uint64_t steps_per_point_bound(float step, float save_at)
+{
+    if (!(step > 0.0f) || !(save_at > 0.0f) || !std::isfinite(step) || !std::isfinite(save_at)) return 0;
+    if (step >= save_at) return 1;   // every iteration saves a point
+    const double s = step;
+    uint64_t count = 1;              // the first iteration: time 0 -> step, exact
+    int e = 0;
+    std::frexp(step, &e);            // step in [2^(e-1), 2^e)
+    double lo = s;
+    while (lo < (double)save_at) {
+        const double hi = std::min(std::ldexp(1.0, e), (double)save_at);
+        // spacing of binary32 values in [2^(e-1), 2^e); subnormal spacing below
+        const double u = std::ldexp(1.0, std::max(e - 24, -149));
+        const double q = std::floor(s / u);
+        const double r = s - q * u;
+        const double inc = (r > 0.5 * u) ? (q + 1.0) * u : q * u;
+        if (inc <= 0.0) return 0;
+        const double n = std::floor((hi - lo) / inc) + 1.0;
+        if (n > 1e18) return 0;
+        count += (uint64_t)n;
+        lo = hi;
+        ++e;
+    }
+    return count;
+}
+
+}  // namespace tg
+
+namespace {
+
+int step_bound(float step, float save_at, uint32_t n_steps, uint64_t* out)
+{
+    const uint64_t per_point = steps_per_point_bound(step, save_at);
+    if (per_point == 0)
+        return fail(TG_ERR_INVALID_ARGUMENT,
+                    "step_size is too small for save_at: in float32, time + step_size no longer "
+                    "reaches save_at, so streamlines would never end");
+    const uint64_t bound = (uint64_t)std::max<uint32_t>(n_steps, 1u) * per_point;
+    if (per_point > 0xffffffffull || bound > 0xffffffffull)
+        return fail(TG_ERR_INVALID_ARGUMENT,
+                    "step_size is too small for save_at and the maximum streamline length: a "
+                    "streamline could take more than 2^32 - 1 steps");
+    *out = bound;
+    return TG_OK;
+}
+
+// make_track_params checks save_at against step_size (the reference's
+// tractogram loop) unless the caller's loop counts steps instead of time
+// (TOD, connectome: tracking.py:181-385, 388-602).
 int make_track_params(const tg_algorithm* a, const tg_domain* d, const tg_field* f, float save_at,
-                      uint32_t n_steps, TrackParams* out)
+                      uint32_t n_steps, TrackParams* out, bool time_loop = true)
 {
     int st = check_algorithm(a);
     if (st != TG_OK) return st;
-    if (d == nullptr || f == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "domain and field are required");
     if (!std::isfinite(save_at) || save_at <= 0.0f)
         return fail(TG_ERR_INVALID_ARGUMENT, "save_at must be finite and positive");
+    uint32_t max_steps = 0xffffffffu;
+    if (time_loop) {
+        uint64_t bound = 0;
+        st = step_bound(a->step_size, save_at, n_steps, &bound);
+        if (st != TG_OK) return st;
+        max_steps = (uint32_t)bound;
+    }
+    if (d == nullptr || f == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "domain and field are required");
     TrackParams p;
     std::memset(&p, 0, sizeof p);
     p.domain_kind = d->d.kind;
@@ -180,6 +252,7 @@ int make_track_params(const tg_algorithm* a, const tg_domain* d, const tg_field*
     p.algo = algo_params(a);
     p.save_at = save_at;
     p.n_steps = n_steps;
+    p.max_steps = max_steps;
     *out = p;
     return TG_OK;
 }
@@ -1197,7 +1270,7 @@ int tg_tod(const tg_algorithm* algorithm, const tg_domain* domain, const tg_fiel
 {
     TodParams q;
     std::memset(&q, 0, sizeof q);
-    int st = make_track_params(algorithm, domain, field, 1.0f, 1u, &q.t);
+    int st = make_track_params(algorithm, domain, field, 1.0f, 1u, &q.t, false);
     if (st != TG_OK) return st;
     if (n_seeds == 0 || n_steps == 0) return TG_OK;
     if (vertices == nullptr || triangles == nullptr || cumulative_areas == nullptr || coefficients == nullptr ||
@@ -1240,7 +1313,7 @@ int tg_connectome(const tg_algorithm* algorithm, const tg_domain* domain, const 
 {
     ConnectomeParams q;
     std::memset(&q, 0, sizeof q);
-    int st = make_track_params(algorithm, domain, field, 1.0f, 1u, &q.t);
+    int st = make_track_params(algorithm, domain, field, 1.0f, 1u, &q.t, false);
     if (st != TG_OK) return st;
     if (n_seeds == 0) return TG_OK;
     if (boundary == nullptr || boundary->d.kind != kDomainMesh)
@@ -1311,6 +1384,16 @@ int tg_update_orientation(int32_t model, uint32_t n_parameters, const tg_algorit
                                      reinterpret_cast<const float4*>(orientations), n,
                                      reinterpret_cast<float4*>(out), as_stream(stream)));
     return TG_OK;
+}
+
+int tg_step_bound(float step_size, float save_at, uint32_t n_steps, uint64_t* max_steps)
+{
+    if (max_steps == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "null argument");
+    if (!std::isfinite(step_size) || step_size <= 0.0f)
+        return fail(TG_ERR_INVALID_ARGUMENT, "step_size must be finite and positive");
+    if (!std::isfinite(save_at) || save_at <= 0.0f)
+        return fail(TG_ERR_INVALID_ARGUMENT, "save_at must be finite and positive");
+    return step_bound(step_size, save_at, n_steps, max_steps);
 }
 
 int tg_rng_stream(int32_t which, uint32_t s0, uint32_t s1, uint32_t n, uint32_t max, void* out, void* stream)

@@ -66,6 +66,11 @@ struct TrackParams {
     AlgoParams algo;
     float save_at;
     uint32_t n_steps;
+    // Upper bound on the steps of one streamline (step_bound in tg_capi.cu):
+    // n_steps saved points times the most loop iterations binary32 time
+    // accumulation can take between two of them.  It never binds for the
+    // inputs the host accepts; it only guarantees that every lane ends.
+    uint32_t max_steps;
 };
 
 // Batched persistent launch over work items 0..n_items-1; item k tracks

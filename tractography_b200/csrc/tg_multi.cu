@@ -143,7 +143,7 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
             break;
         }
         if (!live) continue;
-        bool done = s.n >= P->n_steps;
+        bool done = s.n >= P->n_steps || s.steps >= P->max_steps;
         bool overflow = false;
         if (!done) {
             float qx, qy, qz;

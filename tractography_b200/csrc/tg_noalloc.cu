@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(128) track_persistent_dense_kernel(TrackParams
         lane_init(s, a, b, batch_seeds[batch], local, seed_offset + item);
         float4* line = out + (size_t)item * p.n_steps;
         line[0] = a;
-        while (s.n < p.n_steps) {
+        while (s.n < p.n_steps && s.steps < p.max_steps) {
             float qx, qy, qz;
             const int r = track_step<MODEL, LMAX, ALGO, CPAD>(p, s, c, qx, qy, qz);
             if (r == 0) break;

@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
         }
         budget -= 1u;
         if (!live) continue;
-        bool done = s.n >= J->t.n_steps;
+        bool done = s.n >= J->t.n_steps || s.steps >= J->t.max_steps;
         bool overflow = false;
         if (!done) {
             float qx, qy, qz;

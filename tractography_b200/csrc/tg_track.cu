@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128) track_dense_kernel(TrackParams p, const f
     for (int k = 0; k < CPAD; ++k) c[k] = 0.0f;
     float4* line = out + (size_t)gid * p.n_steps;
     line[0] = a;
-    while (s.n < p.n_steps) {
+    while (s.n < p.n_steps && s.steps < p.max_steps) {
         float qx, qy, qz;
         const int r = track_step<MODEL, LMAX, ALGO, CPAD, DOM>(p, s, c, qx, qy, qz);
         if (r == 0) break;
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
         // all its lanes (warp_leaves_hit); same answers as a test per lane.
         int surface = -1;
         if constexpr (DOM == kDomainMesh) {
-            const bool testing = live && s.n < p.n_steps && s.steps > 0u;
+            const bool testing = live && s.n < p.n_steps && s.steps < p.max_steps && s.steps > 0u;
             uint32_t list = 0;
             int route = 0;
             Segment g;
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
             if (testing) surface = route == 0 ? 0 : (route == 1 ? (hit ? 1 : 0) : -1);
         }
         if (!live) continue;
-        bool done = s.n >= p.n_steps;
+        bool done = s.n >= p.n_steps || s.steps >= p.max_steps;
         bool overflow = false;
         if (!done) {
             float qx, qy, qz;
