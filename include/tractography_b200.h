@@ -296,8 +296,12 @@ int tg_tracker_copy_points(tg_tracker* tracker, float* dst, uint64_t first, uint
  * that holds at most TG_NOALLOC_MAX_BATCHES batch seeds -- more batches are
  * rejected with TG_ERR_INVALID_ARGUMENT.  The first call on a device looks
  * up that array's address (cudaGetSymbolAddress) and should come before any
- * stream capture.  Every call shares the array: calls that overlap on the
- * GPU race and must be serialised by the caller. */
+ * stream capture.  batch_rng_seeds is copied into the array on `stream`:
+ * from pageable host memory the call returns after the copy; from
+ * page-locked memory it may return before, and the caller must leave the
+ * array unchanged until the stream has run the copy.  Every call shares the
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller. */
 int tg_tractogram_noalloc(const tg_algorithm* algorithm, const tg_domain* domain, const tg_field* field,
                           const float* seeds, uint32_t n_seeds, uint32_t batch_size,
                           const uint32_t* batch_rng_seeds, float save_at, uint32_t n_steps, float* streamlines,

@@ -143,3 +143,22 @@ def test_results_spanning_several_segments(runtime):
     for i in range(len(lengths)):
         assert bits_equal(points[offsets[i]:offsets[i] + lengths[i]],
                           alone.points[alone.offsets[i]:alone.offsets[i] + alone.lengths[i]]), i
+
+
+def test_failed_reservation_only_warns(runtime):
+    """A reservation larger than the device fails with a warning, and the
+    server still serves: the failed allocation must not surface as the error
+    of the next epoch's launch."""
+    import torch
+
+    total = torch.cuda.get_device_properties(runtime.device).total_memory
+    job = make_jobs(seed=5)[0]
+    alone = run_alone(job, runtime)
+    with pytest.warns(UserWarning, match="reservation"):
+        server = Server(runtime, hbm_budget_bytes=4e9, epoch_steps=64, reserve_bytes=2 * total)
+    with server:
+        rid = server.submit(job)
+        got = server.drain()[rid]
+    assert np.array_equal(np.array([len(s) for s in got.streamlines]), alone.lengths)
+    for i, s in enumerate(got.streamlines):
+        assert bits_equal(s, alone.points[alone.offsets[i]:alone.offsets[i] + alone.lengths[i]]), i

@@ -6,9 +6,10 @@ device synchronisation -- pass every input and output themselves; the only
 scratch is the library's static device array.  This test calls the entry
 point through the C ABI twice in a row (the array keeps the previous call's
 contents, so the second call checks that the counters are cleared) and
-compares both results with the existing entry points: bit for bit, the
-tolerance every parity test here uses.  It lives in a file of its own that
-pytest collects last, and passes alone in a fresh process or after the rest.
+compares both results with the existing entry points and the first batch
+with the CPU oracle: bit for bit, the tolerance every parity test here
+uses.  It lives in a file of its own that pytest collects last, and passes
+alone in a fresh process or after the rest.
 """
 
 import ctypes
@@ -20,7 +21,7 @@ import tractography_b200 as tg
 from tractography_b200 import _lib
 from tractography_b200.algorithm import to_struct
 
-from helpers import bits_equal, small_config0
+from helpers import bits_equal, oracle_case, small_config0
 
 pytestmark = pytest.mark.gpu
 
@@ -67,6 +68,13 @@ def test_noalloc_matches_existing_entry_points_twice():
             assert np.array_equal(lengths[sl], want_len)
             for i in range(len(want_len)):
                 assert bits_equal(out[sl][i, : want_len[i]], want[i, : want_len[i]]), (call, b, i)
+
+        # and the CPU oracle for the first batch
+        want, want_len = oracle_case(alg, domain, field, rng_seed=int(rng_seeds[0]), save_at=save_at,
+                                     n_steps=n_steps).tractogram(seeds[:batch_size])
+        assert np.array_equal(lengths[:batch_size], want_len)
+        for i in range(len(want_len)):
+            assert bits_equal(out[i, : want_len[i]], want[i, : want_len[i]]), (call, i)
 
         # existing persistent tracker over the same batches
         result = tg.tracking.track_packed(alg, domain, field, seeds, save_at=save_at, n_steps=n_steps,

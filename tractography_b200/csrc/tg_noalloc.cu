@@ -7,7 +7,7 @@
  * synchronise the device) are not acceptable.  For them this file provides
  * tg_tractogram_noalloc(): the persistent lane-refill tracker writing the
  * reference's dense output into caller buffers, whose only scratch memory
- * (a work-item counter, a step counter and the per-batch RNG seeds) lives
+ * (a work-item counter and the per-batch RNG seeds) lives
  * in the file-scope __device__ array below.
  *
  * Properties of that array, which every caller shares:
@@ -18,8 +18,12 @@
  *     address is obtained once per device with cudaGetSymbolAddress, with
  *     that device current, on the first call made on that device; make that
  *     first call before any stream capture.
- *   - Each call clears the counters and overwrites the seeds it uses; the
- *     array otherwise keeps the last call's contents.  Calls that overlap on
+ *   - Each call clears the counter and overwrites the seeds it uses; the
+ *     array otherwise keeps the last call's contents.  The seeds are copied
+ *     from the caller's host array on the call's stream: from pageable
+ *     memory the call returns once they are copied; from page-locked memory
+ *     it may return first, and the host array must then stay unchanged until
+ *     the stream has run the copy.  Calls that overlap on
  *     the GPU (different streams, or host threads on one device) race on it:
  *     serialise them.
  */
@@ -46,7 +50,7 @@ constexpr uint32_t kNoAllocHeaderWords = 64;       // 256 B: counters
 constexpr uint32_t kNoAllocMaxBatches = TG_NOALLOC_MAX_BATCHES;
 constexpr uint32_t kNoAllocWords = kNoAllocHeaderWords + kNoAllocMaxBatches;
 
-// words [0, 2): work-item counter (u64); [2, 4): accepted steps (u64);
+// words [0, 2): work-item counter (u64); [2, 64): unused;
 // [64, 64 + n_batches): per-batch RNG seeds.
 static __device__ __align__(256) uint32_t tg_noalloc_scratch[kNoAllocWords];
 
@@ -63,12 +67,10 @@ __global__ void __launch_bounds__(128) track_persistent_dense_kernel(TrackParams
 {
     constexpr int CPAD = ModelShape<MODEL, LMAX>::CPAD;
     unsigned long long* item_counter = reinterpret_cast<unsigned long long*>(scratch);
-    unsigned long long* steps_done = item_counter + 1;
     const uint32_t* batch_seeds = scratch + kNoAllocHeaderWords;
     float c[CPAD];
 #pragma unroll
     for (int k = 0; k < CPAD; ++k) c[k] = 0.0f;
-    unsigned long long steps_total = 0;
     while (true) {
         const unsigned long long it = atomicAdd(item_counter, 1ull);
         if (it >= n_seeds) break;
@@ -91,9 +93,7 @@ __global__ void __launch_bounds__(128) track_persistent_dense_kernel(TrackParams
             }
         }
         lengths[item] = s.n;
-        steps_total += s.steps;
     }
-    if (steps_total != 0) atomicAdd(steps_done, steps_total);
 }
 
 template <int M, int L, int A>

@@ -1177,7 +1177,16 @@ int tg_server_reserve(tg_server* S, uint64_t bytes)
     // threshold is the budget), so later request buffers are carved from it
     // instead of mapping new memory while requests wait
     void* p = nullptr;
-    TG_STRY(cudaMallocFromPoolAsync(&p, bytes, S->mempool, S->stream));
+    const cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, S->mempool, S->stream);
+    if (e != cudaSuccess) {
+        // A reservation that does not fit only costs time later (the pool
+        // then maps memory as requests need it), so it must not leave its
+        // error as the thread's last CUDA error, where the next launch check
+        // of an epoch would report it.  Drain the stream first, then clear.
+        cudaStreamSynchronize(S->stream);
+        cudaGetLastError();
+        return sfail_cuda(e, "cudaMallocFromPoolAsync (reservation)");
+    }
     TG_STRY(cudaFreeAsync(p, S->stream));
     TG_STRY(cudaStreamSynchronize(S->stream));
     return TG_OK;
