@@ -214,22 +214,9 @@ def replica_seed(rank: int) -> int:
 
 
 def setup_workload(rank: int, n_seeds: int, runtime):
-    import tractography_b200 as tg
     from tractography_b200 import synthetic
 
-    fod = synthetic.config1(seed=0)
-    field = tg.field.Image(fod)
-    mask = np.any(field.values != 0, axis=-1).astype(np.uint8)
-    domain = tg.domain.Image(tg.Nifti1Image(mask, fod.affine))
-    state = np.random.get_state()
-    np.random.seed(replica_seed(rank))
-    try:
-        seeds = tg.seeds.from_fod(fod, n_seeds, runtime=runtime)
-    finally:
-        np.random.set_state(state)
-    model = tg.local.RealSymmetricSphericalHarmonics(C)
-    algorithm = tg.algorithm.Diffusion(model, step_size=STEP, gamma=GAMMA, noise_variance=NOISE, seed=1234 + rank)
-    return fod, field, domain, seeds, algorithm
+    return synthetic.config1_workload(n_seeds, runtime, numpy_seed=replica_seed(rank), algorithm_seed=1234 + rank)
 
 
 def run_ours(args):
@@ -335,6 +322,12 @@ def run_ours(args):
             if dist is not None:
                 dist.barrier()
 
+        # outside the timed region: the last timed run against the oracle
+        parity = None
+        if not args.no_cpu_baseline and world == 1:
+            parity = parity_sample(lib, tracker, sh, algorithm, field, domain, seeds, args.batch,
+                                   rng_seeds[args.warmup + args.steps - 1], lengths, offsets)
+
     if dist is not None:
         (dev_ms, e2e_ms, kernel_ms), (dev_steps, e2e_steps, dev_points, n_launch, n_waves) = combine_ranks(
             dist, [dev_ms, e2e_ms, kernel_ms], [dev_steps, e2e_steps, dev_points, n_launch, n_waves], "cuda")
@@ -402,6 +395,8 @@ def run_ours(args):
                                 "(FFMA = 2); peak = SMs x 128 x 2 x SM clock"}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(field, domain, seeds)
+    if parity is not None:
+        line["parity"] = parity
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -450,6 +445,43 @@ def cpu_baseline(field, domain, seeds, threads=None):
     return {"value": steps / dt, "unit": UNIT, "cores": threads, "kind": kind,
             "sample": f"first {n_sample} seeds of the timed batches ({steps} steps, {dt:.1f} s); {what}; "
                       "pocl unavailable here"}
+
+
+def parity_sample(lib, tracker, stream, algorithm, field, domain, seeds, batch, rng_seeds, lengths, offsets,
+                  n_sample=256, threads=None):
+    """Outside the timed region: the last timed run's streamlines of a spread
+    sample of seeds against the CPU oracle with the same batch RNG seeds and
+    batch-local stream ids (tracking.py:103-148); bit for bit."""
+    from oracle import oracle as O
+    from tractography_b200 import _lib
+
+    threads = threads or os.cpu_count() or 1
+    n = len(seeds)
+    n_steps = int(math.floor(MAX_LENGTH / SAVE_AT))
+    ids = np.unique(np.linspace(0, n - 1, n_sample).astype(np.int64))
+    identical = True
+    mismatches = 0
+    for b in np.unique(ids // batch):
+        sel = ids[ids // batch == b]
+        local = (sel - b * batch).astype(np.uint32)
+        case = O.Case(mask=domain.values, mask_inv_affine=domain.inverse_affine, field=field.values,
+                      field_inv_affine=field.inverse_affine, model=O.MODEL_SH, algorithm=O.ALGO_DIFFUSION,
+                      step_size=algorithm.step_size, gamma=algorithm.gamma,
+                      noise_variance=algorithm.noise_variance, rng_seed=int(rng_seeds[b]), save_at=SAVE_AT,
+                      n_steps=n_steps)
+        want, want_len = case.tractogram_ids(seeds[sel], local, n_threads=threads)
+        for k, i in enumerate(sel):
+            got = np.zeros((int(lengths[i]), 3), np.float32)
+            if len(got):
+                _lib.check(lib.tg_tracker_copy_points(tracker, got.ctypes.data_as(ctypes.c_void_p), int(offsets[i]),
+                                                      int(lengths[i]), 1, stream))
+            same = int(lengths[i]) == int(want_len[k]) and np.array_equal(got, want[k, : want_len[k], :3],
+                                                                          equal_nan=True)
+            if not same:
+                identical = False
+                mismatches += 1
+    return {"seeds": int(len(ids)), "identical": identical, "mismatches": mismatches,
+            "against": "CPU oracle, bit for bit (lengths and every point), last timed run"}
 
 
 def run_reference(args):
@@ -938,17 +970,9 @@ C2_WORKLOAD = ("config2 DTI + mesh: 96x96x60 tensors (6 f32) at 2 mm along the c
 
 
 def setup_config2(runtime, n_seeds):
-    import tractography_b200 as tg
     from tractography_b200 import synthetic
 
-    fod = synthetic.dti_field(shape=(96, 96, 60), seed=0)
-    field = tg.field.Image(fod)
-    v, f = synthetic.config2_surface()
-    mesh = tg.domain.Mesh(v, f)
-    seeds = synthetic.seeds_inside(lambda p: tg.domain.contains(mesh, p, runtime), v.min(axis=0), v.max(axis=0),
-                                   n_seeds, seed=5)
-    algorithm = tg.algorithm.Transport(tg.local.DiffusionTensorImaging(), step_size=C2_STEP, gamma=1.0)
-    return field, mesh, seeds, algorithm
+    return synthetic.config2_workload(n_seeds, runtime, step_size=C2_STEP)
 
 
 def run_config2(args):

@@ -38,6 +38,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 N_STEPS_SENTINEL = 987654
+NNZ_SENTINEL = 54321     # nonzero voxels of the FOD the seeding kernel is captured with
 
 VARIANTS = [
     # name, model, coefficients, algorithm
@@ -71,6 +72,12 @@ class RecordingRuntime:
     def build_program(self, source, options=()):
         self.source = source
         raise _Captured()
+
+    def build_kernel_program(self, names, values=None, *, options=()):
+        # the reference's own loader and templating (opencl.py:86-109), which
+        # ends in build_program above
+        return sys.modules["tractography.opencl"].OpenCLRuntime.build_kernel_program(
+            self, names, values, options=options)
 
 
 def capture(ref, model, n_coefficients, algorithm):
@@ -336,6 +343,64 @@ def capture_connectome(ref, algorithm):
     raise RuntimeError("the reference did not build a program")
 
 
+FOD_SEED_VARIANTS = [("fodseed_sh45", "sh", 45), ("fodseed_dti", "dti", 6)]
+
+FOD_SEED_DRIVER = """
+extern "C" void tgref_{name}(const float* fod, const float* voxels, const float* affine, unsigned int* states,
+        float* seeds, unsigned int nnz, unsigned int n, int threads)
+{{
+    tgref_nnz = nnz;
+    long g;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : 1)
+    for (g = 0; g < (long)n; ++g) {{
+        tgref_global_id = (size_t)g;
+        {name}::seeds_from_fod((const float (*)[{C}])fod, (const float4*)voxels, (const float4*)affine,
+                               (uint2*)states, (float4 (*)[2])seeds);
+    }}
+}}
+"""
+
+
+def capture_fod_seeds(ref, n_coefficients):
+    """The FOD seeding kernel as seeds.from_fod assembles it (seeds.py:174-216,
+    utils/seeds.cl), for a volume of NNZ_SENTINEL nonzero voxels."""
+    Image = sys.modules["nibabel.nifti1"].Nifti1Image
+    fod = Image(np.ones((NNZ_SENTINEL, 1, 1, n_coefficients), np.float32), np.eye(4))
+    rt = RecordingRuntime()
+    state = np.random.get_state()
+    try:
+        ref.seeds.from_fod(fod, 4, runtime=rt)
+    except _Captured:
+        return rt.source
+    finally:
+        np.random.set_state(state)
+    raise RuntimeError("the reference did not build a program")
+
+
+def fod_seed_source(ref, kernel_dir, name, n_coefficients):
+    src = capture_fod_seeds(ref, n_coefficients)
+    # the voxel count is a template value in the kernel (randi(state, $nnz));
+    # make it the driver's run-time value (array bounds keep the sentinel,
+    # they are pointers once the kernel is compiled)
+    call = f"randi(state, {NNZ_SENTINEL})"
+    if src.count(call) != 1:
+        raise RuntimeError("unexpected seeding kernel source")
+    src = src.replace(call, "randi(state, tgref_nnz)")
+    cpp = to_cpp(src, kernel_dir, name).replace("extern unsigned int tgref_n_steps;",
+                                                  "extern unsigned int tgref_nnz;")
+    # utils/seeds.cl:94 draws the x, y and z jitter inside one vector
+    # literal; as make_float4 arguments g++ would draw them right to left, so
+    # sequence them left to right as clang (pocl) evaluates the initialiser
+    jitter = re.compile(r"voxel\s*\+=\s*make_float4\(randu\(state\)\s*-\s*0\.5f,\s*randu\(state\)\s*-\s*0\.5f,"
+                        r"\s*randu\(state\)\s*-\s*0\.5f,\s*0\.0f\);")
+    cpp, n = jitter.subn("{ const float tgref_j0 = randu(state) - 0.5f; const float tgref_j1 = randu(state) - 0.5f; "
+                         "const float tgref_j2 = randu(state) - 0.5f; voxel += make_float4(tgref_j0, tgref_j1, "
+                         "tgref_j2, 0.0f); }", cpp)
+    if n != 1:
+        raise RuntimeError("unexpected seeding kernel source (jitter draw)")
+    return cpp + FOD_SEED_DRIVER.format(name=name, C=n_coefficients)
+
+
 def bvh_source(kernel_dir):
     """utils/bvh.cl (the boundary BVH traversal) as C++ with a batch driver."""
     text = rewrite_literals(inline_includes((kernel_dir / "utils" / "bvh.cl").read_text(), kernel_dir))
@@ -358,7 +423,7 @@ def main():
     objects = []
     common = OUT / "tgref_common.cpp"
     common.write_text('#include <cstddef>\nthread_local size_t tgref_global_id;\nunsigned int tgref_n_steps;\n'
-                      'thread_local unsigned long long tgref_steps;\n')
+                      'thread_local unsigned long long tgref_steps;\nunsigned int tgref_nnz;\n')
     sources = [common]
     for name, model, C, algorithm in VARIANTS:
         src = capture(ref, model, C, algorithm)
@@ -385,6 +450,10 @@ def main():
             path.write_text(to_cpp(capture_fn(ref, algorithm), kernel_dir, tname) +
                             driver.format(name=tname, noise_arg=noise_arg))
             sources.append(path)
+    for name, _model, C in FOD_SEED_VARIANTS:
+        path = OUT / f"tgref_{name}.cpp"
+        path.write_text(fod_seed_source(ref, kernel_dir, name, C))
+        sources.append(path)
     spath = OUT / "tgref_seed.cpp"
     spath.write_text(to_cpp(capture_seed(ref), kernel_dir, "seedref").replace(
         "extern unsigned int tgref_n_steps;", "") + SEED_DRIVER)
@@ -395,7 +464,11 @@ def main():
     for src in sources:
         obj = src.with_suffix(".o")
         objects.append(obj)
-        procs.append(subprocess.Popen(["g++", *flags, "-c", str(src), "-o", str(obj)]))
+        # OpenCL C passes `const float fod[]` to a `float*` parameter
+        # (utils/seeds.cl:40 into the models' evaluate_interpolated_model);
+        # C++ needs -fpermissive to accept that conversion
+        extra = ["-fpermissive"] if src.name.startswith("tgref_fodseed_") else []
+        procs.append(subprocess.Popen(["g++", *flags, *extra, "-c", str(src), "-o", str(obj)]))
     if any(p.wait() != 0 for p in procs):
         raise SystemExit("compiling the reference kernels failed")
     subprocess.run(["g++", "-shared", "-fopenmp", "-o", str(OUT / "libtgref.so"), *map(str, objects)], check=True)

@@ -73,6 +73,8 @@ def lib():
         U32, I32, F = ctypes.c_uint32, ctypes.c_int32, ctypes.c_float
         _lib.tgo_tractogram.argtypes = [P, P, U32, P, P, ctypes.c_int]
         _lib.tgo_tractogram.restype = ctypes.c_uint64
+        _lib.tgo_tractogram_ids.argtypes = [P, P, P, U32, P, P, ctypes.c_int]
+        _lib.tgo_tractogram_ids.restype = ctypes.c_uint64
         _lib.tgo_contains.argtypes = [P, P, U32, P]
         _lib.tgo_field_evaluate.argtypes = [P, P, U32, P]
         _lib.tgo_local_evaluate.argtypes = [I32, U32, P, P, U32, P]
@@ -138,6 +140,20 @@ class Case:
         out = np.zeros((n, self.p.n_steps, 4), dtype=np.float32)
         lengths = np.zeros(n, dtype=np.uint32)
         steps = lib().tgo_tractogram(ctypes.byref(self.p), _ptr(seeds), n, _ptr(out), _ptr(lengths), n_threads)
+        if return_steps:
+            return out, lengths, int(steps)
+        return out, lengths
+
+    def tractogram_ids(self, seeds, ids, n_threads=1, return_steps=False):
+        """Seeds taken out of a larger call: seed k is work item ids[k] of it."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        n = seeds.shape[0]
+        assert ids.shape == (n,)
+        out = np.zeros((n, self.p.n_steps, 4), dtype=np.float32)
+        lengths = np.zeros(n, dtype=np.uint32)
+        steps = lib().tgo_tractogram_ids(ctypes.byref(self.p), _ptr(seeds), _ptr(ids), n, _ptr(out), _ptr(lengths),
+                                         n_threads)
         if return_steps:
             return out, lengths, int(steps)
         return out, lengths

@@ -175,3 +175,25 @@ def connectome(domain, field, bvh, algorithm_kind, step, gamma, noise, rng_seed,
     fn.argtypes = types + [ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
     fn(*args, minimum_length, rows.ctypes.data, cols.ctypes.data, w.ctypes.data, threads)
     return rows, cols, w
+
+
+def seeds_from_fod(model, fod_sparse, voxels, affine, states, threads=1):
+    """The reference's FOD seeding kernel (utils/seeds.cl:99-118 as seeds.py:174-216
+    builds it) on the CPU: sparse (nnz, C) coefficients, (nnz, 4) voxel indices,
+    the float32 voxel-to-world affine and (n, 2) MWC64X states.  Returns the
+    (n, 8) seeds and the states after the draws."""
+    C = 6 if model == "dti" else 45
+    fod_sparse = np.ascontiguousarray(fod_sparse, dtype=np.float32)
+    assert fod_sparse.shape[1] == C
+    voxels = np.ascontiguousarray(voxels, dtype=np.float32)
+    affine = np.ascontiguousarray(affine, dtype=np.float32)
+    states = np.array(states, dtype=np.uint32, order="C", copy=True)
+    n = states.shape[0]
+    seeds = np.zeros((n, 8), np.float32)
+    fn = getattr(lib(), "tgref_fodseed_" + ("dti" if model == "dti" else "sh45"))
+    P = ctypes.c_void_p
+    fn.argtypes = [P, P, P, P, P, ctypes.c_uint, ctypes.c_uint, ctypes.c_int]
+    fn.restype = None
+    fn(fod_sparse.ctypes.data, voxels.ctypes.data, affine.ctypes.data, states.ctypes.data, seeds.ctypes.data,
+       len(voxels), n, threads)
+    return seeds, states

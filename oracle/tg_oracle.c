@@ -839,6 +839,25 @@ uint64_t tgo_tractogram(const tgo_problem* p, const float* seeds, uint32_t n_see
     return total;
 }
 
+uint64_t tgo_tractogram_ids(const tgo_problem* p, const float* seeds, const uint32_t* ids, uint32_t n_seeds,
+                            float* streamlines, uint32_t* lengths, int n_threads)
+{
+    if (p->n_steps == 0) {
+        for (uint32_t i = 0; i < n_seeds; ++i) lengths[i] = 0;
+        return 0;
+    }
+    uint64_t total = 0;
+    long i;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total) num_threads(n_threads > 0 ? n_threads : 1)
+    for (i = 0; i < (long)n_seeds; ++i) {
+        float* out = streamlines + (size_t)i * p->n_steps * 4;
+        uint64_t steps = 0;
+        lengths[i] = track_one(p, seeds + 8 * (size_t)i, ids[i], out, &steps);
+        total += steps;
+    }
+    return total;
+}
+
 void tgo_contains(const tgo_problem* p, const float* points, uint32_t n, uint8_t* out)
 {
     for (uint32_t i = 0; i < n; ++i)

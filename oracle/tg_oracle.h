@@ -75,6 +75,12 @@ typedef struct {
 uint64_t tgo_tractogram(const tgo_problem* p, const float* seeds, uint32_t n_seeds,
                         float* streamlines, uint32_t* lengths, int n_threads);
 
+/* tgo_tractogram for seeds taken out of a larger call: seed i is work item
+ * ids[i] of that call (tracking.py:103 get_global_id, which keys its
+ * rng_init stream and its Philox counter). */
+uint64_t tgo_tractogram_ids(const tgo_problem* p, const float* seeds, const uint32_t* ids, uint32_t n_seeds,
+                            float* streamlines, uint32_t* lengths, int n_threads);
+
 /* domain.py:358-382 for n points (x, y, z, w) -> 0/1. */
 void tgo_contains(const tgo_problem* p, const float* points, uint32_t n, uint8_t* out);
 

@@ -49,3 +49,43 @@ def small_config0(n_voxels=16, n_seeds=200, seed=1):
     fod, mask = synthetic.config0(n=n_voxels)
     seeds = synthetic.seeds_in_mask(mask, n_seeds, seed=seed)
     return tg.field.Image(fod), tg.domain.Image(mask), seeds
+
+
+def tracker_run_sampled(runtime, algorithm, domain, field, seeds, *, save_at, n_steps, batch_size,
+                        batch_rng_seeds, sample):
+    """One tg_tracker_run over every seed (seeds resident on the device), then
+    the points of the sampled seeds only.
+
+    Returns (lengths of all seeds, accepted steps, total points, {seed: points})."""
+    import ctypes
+
+    from tractography_b200 import _lib
+    from tractography_b200.algorithm import to_struct
+    from tractography_b200.tracking import _handles
+
+    n = int(seeds.shape[0])
+    rng = np.ascontiguousarray(batch_rng_seeds, dtype=np.uint32)
+    lengths = np.empty(n, np.uint32)
+    offsets = np.empty(n, np.uint64)
+    total, steps = ctypes.c_uint64(), ctypes.c_uint64()
+    sh = ctypes.c_void_p(runtime.stream_handle)
+    with runtime.device_scope():
+        d_handle, f_handle = _handles(algorithm, domain, field, runtime)
+        a = to_struct(algorithm)
+        d_seeds = runtime.to_device(np.ascontiguousarray(seeds, np.float32))
+        tracker = runtime.tracker()
+        _lib.check(runtime.lib.tg_tracker_run(
+            tracker, ctypes.byref(a), d_handle, f_handle, ctypes.c_void_p(d_seeds.data_ptr()), 0, n, int(batch_size),
+            rng.ctypes.data_as(ctypes.c_void_p), float(save_at), int(n_steps), lengths.ctypes.data_as(ctypes.c_void_p),
+            offsets.ctypes.data_as(ctypes.c_void_p), ctypes.byref(total), ctypes.byref(steps), sh))
+        points = {}
+        for i in sample:
+            i = int(i)
+            buf = np.zeros((int(lengths[i]), 3), np.float32)
+            if len(buf):
+                _lib.check(runtime.lib.tg_tracker_copy_points(tracker, buf.ctypes.data_as(ctypes.c_void_p),
+                                                              int(offsets[i]), int(lengths[i]), 1, sh))
+            points[i] = buf
+        runtime.finish()
+        del d_seeds
+    return lengths, int(steps.value), int(total.value), points

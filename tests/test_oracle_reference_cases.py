@@ -264,3 +264,22 @@ def test_seed_orientations_follow_the_fod(kind):
     o = seeds[:, 4:7]
     np.testing.assert_allclose(np.einsum("ni,nj->ij", o, o) / len(o), expected, atol=2e-2)
     assert np.all(np.abs(seeds[:, :3]) <= 0.5)
+
+
+def test_oracle_tractogram_ids_keys_streams_by_work_item():
+    """A seed taken out of a larger call keeps that call's stream (rng_init(rng_seed, gid),
+    core.cl:203-208): tractogram_ids on a subset equals the full call's rows."""
+    from helpers import oracle_case, small_config0
+
+    field, domain, seeds = small_config0(n_voxels=12, n_seeds=60, seed=4)
+    alg = tg.algorithm.Diffusion(tg.local.RealSymmetricSphericalHarmonics(45), step_size=0.1, gamma=1.0,
+                                 noise_variance=0.1, seed=3)
+    c = oracle_case(alg, domain, field, rng_seed=99, save_at=0.25, n_steps=40)
+    full, full_len = c.tractogram(seeds)
+    ids = np.array([59, 3, 17, 40, 0], np.uint32)
+    part, part_len = c.tractogram_ids(seeds[ids], ids)
+    assert np.array_equal(part_len, full_len[ids])
+    assert np.array_equal(part, full[ids], equal_nan=True)
+    # the stream follows the id, not the position in the call
+    other, _ = c.tractogram(seeds[ids])
+    assert not np.array_equal(other, part, equal_nan=True)

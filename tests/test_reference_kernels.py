@@ -184,3 +184,42 @@ def test_diffusion_tod_and_connectome_within_reference_sampling_noise():
     T2 = R.tod(domain, field, bvh, "diffusion", 0.1, 1.0, 0.05, 100, 20000, 80, (12, 12, 3), np.eye(4), threads=8)
     T3 = case.tod(domain.boundary_arrays(), 20000, 80, (12, 12, 3), np.eye(4))
     assert np.abs(T1 - T3).sum() < np.abs(T1 - T2).sum()
+
+
+@pytest.mark.parametrize("model", ["sh", "dti"])
+def test_fod_seeding_matches_reference_kernel(model):
+    """seeds.from_fod (seeds.py:174-216) on the reference's own seeds.cl kernel vs
+    the oracle, on identical MWC64X states drawn as the reference draws them
+    (np.random.randint(4294967295, size=(n, 2)), seeds.py:185).
+
+    * voxel choice and jitter (seeds.cl:89-94) are integer and exact float
+      arithmetic: the world locations agree bit for bit for every seed;
+    * the orientation is the first of 1000 Fibonacci directions whose
+      cumulative softplus'd model value exceeds a uniform threshold
+      (seeds.cl:29-56).  The same direction is chosen for >= 99.9 % of seeds,
+      and where one differs it is the neighbouring direction in the
+      cumulative order (the sums round differently at the threshold);
+    * the chosen directions agree to 2.4e-7 (the reference's sincos/sqrt come
+      from the platform's libm, the oracle's from tg_fmath.h).
+
+    The GPU tests then pin the CUDA seeding to the oracle bit for bit."""
+    if model == "sh":
+        fod, _ = synthetic.config0(n=16)
+    else:
+        fod = synthetic.dti_field(shape=(24, 24, 16), seed=4)
+    inline, voxels, affine = tg.seeds.sparse_fod(fod)
+    states = np.random.RandomState(11).randint(4294967295, size=(4000, 2)).astype(np.uint32)
+    ref, ref_states = R.seeds_from_fod(model, inline, voxels, affine, states, threads=4)
+    ours = O.seeds_from_fod(O.MODEL_DTI if model == "dti" else O.MODEL_SH, inline, voxels, affine, states,
+                            n_threads=4)
+    assert np.array_equal(ref[:, :4].view(np.uint32), ours[:, :4].view(np.uint32))
+    assert np.all(ref[:, 7] == 0.0) and np.all(ours[:, 7] == 0.0)
+    fib = synthetic.fibonacci(1000)
+    i_ref = np.argmax(ref[:, 4:7] @ fib.T, axis=1)
+    i_ours = np.argmax(ours[:, 4:7] @ fib.T, axis=1)
+    same = i_ref == i_ours
+    assert same.mean() >= 0.999, same.mean()
+    assert np.all(np.abs(i_ref[~same] - i_ours[~same]) == 1), (i_ref[~same], i_ours[~same])
+    assert np.abs(ref[same, 4:7] - ours[same, 4:7]).max() <= 2.4e-7
+    # the kernel writes back the states after its draws (seeds.cl:117)
+    assert not np.array_equal(ref_states, states)

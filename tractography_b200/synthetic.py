@@ -393,3 +393,54 @@ def seeds_inside(contains, bounds_lo, bounds_hi, n: int, seed: int = 0, chunk: i
     out = np.empty((n, 8), np.float32)
     out[:, :3], out[:, 3], out[:, 4:7], out[:, 7] = loc, 1.0, o, 0.0
     return out
+
+
+def config1_workload(n_seeds: int, runtime, *, numpy_seed: int = 2024, algorithm_seed: int = 1234):
+    """The single-volume Diffusion job: the 145x174x145 lmax-8 volume of
+    ``config1(seed=0)``, its nonzero voxels as the domain, ``n_seeds`` seeds
+    from ``seeds.from_fod`` under ``numpy.random.seed(numpy_seed)`` (the
+    global RNG is restored afterwards), and Diffusion with step 0.001 mm,
+    gamma 1, noise variance 0.1 seeded by ``algorithm_seed``.
+
+    Returns (fod image, field, domain, seeds, algorithm)."""
+    from . import algorithm as _algorithm
+    from . import domain as _domain
+    from . import field as _field
+    from . import local as _local
+    from . import seeds as _seeds
+
+    fod = config1(seed=0)
+    field = _field.Image(fod)
+    mask = np.any(field.values != 0, axis=-1).astype(np.uint8)
+    domain = _domain.Image(Nifti1Image(mask, fod.affine))
+    state = np.random.get_state()
+    np.random.seed(numpy_seed)
+    try:
+        seeds = _seeds.from_fod(fod, n_seeds, runtime=runtime)
+    finally:
+        np.random.set_state(state)
+    model = _local.RealSymmetricSphericalHarmonics(45)
+    algorithm = _algorithm.Diffusion(model, step_size=0.001, gamma=1.0, noise_variance=0.1, seed=algorithm_seed)
+    return fod, field, domain, seeds, algorithm
+
+
+def config2_workload(n_seeds: int, runtime, *, step_size: float = 0.2):
+    """The tensor job in a closed-surface domain: 96x96x60 tensors at 2 mm
+    (``dti_field(seed=0)``), the ~499k-triangle surface of
+    ``config2_surface()``, ``n_seeds`` seeds uniform inside it (seed 5) and
+    Transport at 0.1 voxel.
+
+    Returns (field, mesh domain, seeds, algorithm)."""
+    from . import algorithm as _algorithm
+    from . import domain as _domain
+    from . import field as _field
+    from . import local as _local
+
+    fod = dti_field(shape=(96, 96, 60), seed=0)
+    field = _field.Image(fod)
+    v, f = config2_surface()
+    mesh = _domain.Mesh(v, f)
+    seeds = seeds_inside(lambda p: _domain.contains(mesh, p, runtime), v.min(axis=0), v.max(axis=0), n_seeds,
+                         seed=5)
+    algorithm = _algorithm.Transport(_local.DiffusionTensorImaging(), step_size=step_size, gamma=1.0)
+    return field, mesh, seeds, algorithm
