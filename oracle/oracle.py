@@ -261,7 +261,8 @@ def philox(counter, key):
 def math(which, x):
     x = np.ascontiguousarray(x, dtype=np.float32)
     out = np.zeros_like(x)
-    code = {"sin": 0, "cos": 1, "exp": 2, "log": 3}[which]
+    code = {"sin": 0, "cos": 1, "exp": 2, "log": 3, "exps2_cos": 4, "exps2_sinc": 5, "softplus": 6,
+            "softplus_slope": 7}[which]
     lib().tgo_math(code, _ptr(x), x.size, _ptr(out))
     return out
 

@@ -22,6 +22,7 @@
 
 #define N_DIRECTIONS 1000
 #define SOFTMAX_SCALE 100.0f
+#define SOFTMAX_INV_SCALE 0x1.47ae14p-7f   /* 1/100 rounded */
 
 /* OpenCL max()/min() on floats (x < y ? y : x), core to the reference's
  * max(value, 1e-6f) and max(value, 0.0f). */
@@ -242,10 +243,6 @@ static float softmax(float x, float k)
     return x;
 }
 
-static float dsoftmax(float x, float k)
-{
-    return 1.0f / (1.0f + tgm_expf(-k * x));
-}
 
 /* local.py:91-120 */
 static model_value_t sh_model(const float* params, uint32_t n_params, frame_t f)
@@ -255,8 +252,9 @@ static model_value_t sh_model(const float* params, uint32_t n_params, frame_t f)
     const int full = (lmax + 1) * (lmax + 2) / 2;
     for (int i = 0; i < full; ++i) c[i] = (uint32_t)i < n_params ? params[i] : 0.0f;
     model_value_t r = sh_raw(c, lmax, f);
-    const float d = dsoftmax(r.value, SOFTMAX_SCALE);
-    r.value = softmax(r.value, SOFTMAX_SCALE);
+    /* core.cl:111-120 softmax and dsoftmax from one exponential */
+    float d;
+    tgm_softplus(r.value, SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &r.value, &d);
     r.dtheta = r.dtheta * d;
     r.dphi = r.dphi * d;
     return r;
@@ -295,11 +293,10 @@ typedef struct {
 
 static void exps2(float o[3], const float t[3])      /* core.cl:101-109 */
 {
-    const float n = sqrtf(fmaf(t[2], t[2], fmaf(t[1], t[1], t[0] * t[0])));
-    if (n <= 0.0f) return;
-    float s, c;
-    tgm_sincosf(n, &s, &c);
-    const float k = s / n;
+    const float n2 = fmaf(t[2], t[2], fmaf(t[1], t[1], t[0] * t[0]));
+    if (n2 <= 0.0f) return;
+    float c, k;
+    tgm_exps2_factors(n2, &c, &k);
     o[0] = fmaf(t[0], k, c * o[0]);
     o[1] = fmaf(t[1], k, c * o[1]);
     o[2] = fmaf(t[2], k, c * o[2]);
@@ -1049,6 +1046,10 @@ void tgo_math(int which, const float* x, uint32_t n, float* out)
         case 1: out[i] = tgm_cosf(x[i]); break;
         case 2: out[i] = tgm_expf(x[i]); break;
         case 3: out[i] = tgm_logf(x[i]); break;
+        case 4: { float c, k; tgm_exps2_factors(x[i], &c, &k); out[i] = c; } break;
+        case 5: { float c, k; tgm_exps2_factors(x[i], &c, &k); out[i] = k; } break;
+        case 6: { float v, d; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d); out[i] = v; } break;
+        case 7: { float v, d; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d); out[i] = d; } break;
         default: out[i] = x[i]; break;
         }
     }

@@ -37,6 +37,39 @@ def test_exp_within_two_ulp(oracle):
     assert special[0] == 1.0 and special[1] == 0.0 and np.isinf(special[2]) and np.isnan(special[3])
 
 
+def test_exps2_factors_within_two_ulp(oracle):
+    """cos(n) and sin(n)/n from n2 = n^2 (the exponential map, core.cl:101-109): the
+    series below n2 = 1 and the general path above agree with float64 to 2 ulp."""
+    series = np.concatenate([np.linspace(1e-12, 1.0, 1_000_001, dtype=np.float32)[:-1],
+                             np.array([np.nextafter(np.float32(1.0), np.float32(0.0))], np.float32)])
+    n = np.sqrt(series.astype(np.float64))
+    assert ulp_error(oracle.math("exps2_cos", series), np.cos(n)).max() <= 2.0
+    assert ulp_error(oracle.math("exps2_sinc", series), np.sin(n) / n).max() <= 2.0
+    # above n2 = 1: sin and cos of n = sqrt(n2) rounded to binary32
+    general = np.linspace(1.0, 400.0, 400_001, dtype=np.float32)
+    n32 = np.sqrt(general).astype(np.float64)
+    assert ulp_error(oracle.math("exps2_cos", general), np.cos(n32)).max() <= 2.0
+    assert ulp_error(oracle.math("exps2_sinc", general), np.sin(n32) / n32).max() <= 3.0
+
+
+def test_softplus_and_slope(oracle):
+    """softplus(x) = log(1 + e^{100x})/100 below 100x = 30, else x; slope 1/(1 + e^{-100x})
+    (core.cl:111-120), both from one exponential."""
+    x = np.linspace(-1.2, 0.6, 1_000_001, dtype=np.float32)
+    x64 = x.astype(np.float64)
+    want = np.where(100 * x64 < 30, np.log1p(np.exp(100 * x64)) / 100, x64)
+    got = oracle.math("softplus", x).astype(np.float64)
+    # log(1 + E) inherits the rounding of the binary32 sum 1 + E (half an ulp
+    # of 1, divided by 100), as the reference's formula does; beyond that 3 ulp
+    allowed = 3 * np.spacing(want.astype(np.float32)).astype(np.float64) + 2.0 ** -24 / 100 * 1.01
+    assert np.all(np.abs(got - want) <= allowed)
+    slope = oracle.math("softplus_slope", x)
+    want_slope = 1 / (1 + np.exp(-100 * x64))
+    assert np.abs(slope - want_slope).max() <= 4 * np.spacing(np.float32(1.0))
+    assert np.all(slope[100 * x >= 30] == 1.0)
+    assert np.isnan(oracle.math("softplus_slope", np.array([np.nan], np.float32))[0])
+
+
 def test_log_within_two_ulp(oracle):
     rng = np.random.default_rng(0)
     x = np.concatenate([

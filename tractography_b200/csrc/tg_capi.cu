@@ -245,8 +245,11 @@ int make_track_params(const tg_algorithm* a, const tg_domain* d, const tg_field*
     } else {
         p.dgrid = grid_of(d->d.inv_affine, d->d.nx, d->d.ny, d->d.nz);
         p.mask = d->d.mask;
+        // one voxel test serves both images (tg_step.cuh locate) for axes
+        // below 2^22 voxels, where voxel index +- 0.5 is exact in binary32
         p.same_grid = d->d.nx == f->d.nx && d->d.ny == f->d.ny && d->d.nz == f->d.nz &&
-                      std::memcmp(d->d.inv_affine, f->d.inv_affine, 12 * sizeof(float)) == 0;
+                      std::memcmp(d->d.inv_affine, f->d.inv_affine, 12 * sizeof(float)) == 0 &&
+                      f->d.nx < (1u << 22) && f->d.ny < (1u << 22) && f->d.nz < (1u << 22);
     }
     p.algorithm = a->algorithm;
     p.algo = algo_params(a);

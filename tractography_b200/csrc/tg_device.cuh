@@ -26,6 +26,7 @@
 namespace tg {
 
 constexpr float kSoftmaxScale = 100.0f;   // local.py:17
+constexpr float kSoftmaxInvScale = 0x1.47ae14p-7f;   // 1/100 rounded
 
 template <int LMAX>
 __device__ __forceinline__ void sh_eval(const float* c, float ct, float st, float cp, float sp,
@@ -172,24 +173,21 @@ struct ModelValue {
     float value, dtheta, dphi;
 };
 
-__device__ __forceinline__ float softmax(float x, float k)   // core.cl:111-115
+// core.cl:111-115 (the seeding kernel's model value; tracking uses tgm_softplus)
+__device__ __forceinline__ float softmax(float x, float k)
 {
     if (x * k < 30.0f) return tgm_logf(1.0f + tgm_expf(k * x)) / k;
     return x;
-}
-
-__device__ __forceinline__ float dsoftmax(float x, float k)  // core.cl:118-120
-{
-    return 1.0f / (1.0f + tgm_expf(-k * x));
 }
 
 template <int LMAX>
 __device__ __forceinline__ ModelValue sh_model(const float* c, const Frame& f)
 {
     ModelValue r;
-    sh_eval<LMAX>(c, f.ct, f.st, f.cp, f.sp, &r.value, &r.dtheta, &r.dphi);
-    const float d = dsoftmax(r.value, kSoftmaxScale);
-    r.value = softmax(r.value, kSoftmaxScale);
+    float raw, d;
+    sh_eval<LMAX>(c, f.ct, f.st, f.cp, f.sp, &raw, &r.dtheta, &r.dphi);
+    // local.py:106-118: softplus of the value, derivatives times its slope
+    tgm_softplus(raw, kSoftmaxScale, kSoftmaxInvScale, &r.value, &d);
     r.dtheta = r.dtheta * d;
     r.dphi = r.dphi * d;
     return r;
@@ -238,11 +236,10 @@ struct RngState {
 
 __device__ __forceinline__ void exps2(float& ox, float& oy, float& oz, float tx, float ty, float tz)
 {
-    const float n = sqrtf(fmaf(tz, tz, fmaf(ty, ty, tx * tx)));
-    if (n <= 0.0f) return;
-    float s, c;
-    tgm_sincosf(n, &s, &c);
-    const float k = s / n;
+    const float n2 = fmaf(tz, tz, fmaf(ty, ty, tx * tx));
+    if (n2 <= 0.0f) return;
+    float c, k;
+    tgm_exps2_factors(n2, &c, &k);
     ox = fmaf(tx, k, c * ox);
     oy = fmaf(ty, k, c * oy);
     oz = fmaf(tz, k, c * oz);

@@ -198,4 +198,58 @@ TGM_FN float tgm_logf(float x_in)
     return (x_in != x_in) ? x_in : result;
 }
 
+/*
+ * The exponential map's factors (core.cl:101-109) from n2 = |t|^2 > 0:
+ * c = cos(n) and k = sin(n) / n with n = sqrt(n2).  For n2 < 1 both are
+ * Taylor series in n2 (cos to n^12, sin(n)/n to n^12 / 13!; truncation
+ * below 1.2e-11), which needs neither the square root, the range reduction
+ * nor the division; larger angles take the general path.
+ */
+TGM_FN void tgm_exps2_factors(float n2, float* c_out, float* k_out)
+{
+    if (n2 < 1.0f) {
+        float pc = 0x1.1eed8ep-29f;                 /*  1/12! */
+        pc = fmaf(pc, n2, -0x1.27e4fcp-22f);        /* -1/10! */
+        pc = fmaf(pc, n2, 0x1.a01a02p-16f);         /*  1/8!  */
+        pc = fmaf(pc, n2, -0x1.6c16c2p-10f);        /* -1/6!  */
+        pc = fmaf(pc, n2, 0x1.555556p-5f);          /*  1/4!  */
+        pc = fmaf(pc, n2, -0.5f);                   /* -1/2!  */
+        *c_out = fmaf(pc, n2, 1.0f);
+        float pk = 0x1.612462p-33f;                 /*  1/13! */
+        pk = fmaf(pk, n2, -0x1.ae6456p-26f);        /* -1/11! */
+        pk = fmaf(pk, n2, 0x1.71de3ap-19f);         /*  1/9!  */
+        pk = fmaf(pk, n2, -0x1.a01a02p-13f);        /* -1/7!  */
+        pk = fmaf(pk, n2, 0x1.111112p-7f);          /*  1/5!  */
+        pk = fmaf(pk, n2, -0x1.555556p-3f);         /* -1/3!  */
+        *k_out = fmaf(pk, n2, 1.0f);
+    } else {
+        const float n = sqrtf(n2);
+        float s, c;
+        tgm_sincosf(n, &s, &c);
+        *c_out = c;
+        *k_out = s / n;
+    }
+}
+
+/*
+ * softplus(x) = log(1 + e^{kx}) / k for kx < 30 (else x) and its derivative
+ * 1 / (1 + e^{-kx}) (core.cl:111-120), from one exponential: with
+ * E = e^{kx} the derivative is E / (1 + E).  For kx >= 30 the derivative
+ * rounds to 1 in binary32 (e^{-30} < 2^-24), and NaN propagates.  The
+ * division by k is a multiplication by inv_k = 1/k rounded.
+ */
+TGM_FN void tgm_softplus(float x, float k, float inv_k, float* value, float* derivative)
+{
+    const float kx = x * k;
+    if (kx < 30.0f) {
+        const float e = tgm_expf(kx);
+        const float one_e = 1.0f + e;
+        *value = tgm_logf(one_e) * inv_k;
+        *derivative = e / one_e;
+    } else {
+        *value = x;
+        *derivative = (kx == kx) ? 1.0f : kx;
+    }
+}
+
 #endif /* TG_FMATH_H */

@@ -32,10 +32,13 @@ struct Lane {
     float time;
     uint32_t n;
     RngState rng;
-    // rounded voxel coordinates of the last domain test and field gather;
-    // while they are unchanged the mask bit (inside) and the coefficients in
-    // registers are still valid, so the bounds tests, index arithmetic and
-    // loads are skipped.  NaN forces the first evaluation.
+    // Voxel cache of the last domain test and field gather; while it holds,
+    // the mask bit (inside) and the coefficients in registers are still
+    // valid, so the voxel rounding, bounds tests, index arithmetic and loads
+    // are skipped.  Domain and field on one grid: the open interval
+    // (dv, fv) per axis in which both voxels are unchanged.  Otherwise (and
+    // for closed surfaces, fv only): the rounded voxel coordinates of the
+    // domain test (dv) and the field gather (fv).  NaN forces an evaluation.
     float dvx, dvy, dvz;
     float fvx, fvy, fvz;
     uint32_t steps;
@@ -83,13 +86,50 @@ __device__ __forceinline__ bool locate(const TrackParams& p, Lane& s, float (&c)
         ax = dot4(p.dgrid.row0, s.px, s.py, s.pz, 1.0f);
         ay = dot4(p.dgrid.row1, s.px, s.py, s.pz, 1.0f);
         az = dot4(p.dgrid.row2, s.px, s.py, s.pz, 1.0f);
-        const float vx = floorf(ax + 0.5f), vy = floorf(ay + 0.5f), vz = floorf(az + 0.5f);
-        float bx = ax, by = ay, bz = az;
-        if (!p.same_grid) {
-            bx = dot4(p.fgrid.row0, s.px, s.py, s.pz, 1.0f);
-            by = dot4(p.fgrid.row1, s.px, s.py, s.pz, 1.0f);
-            bz = dot4(p.fgrid.row2, s.px, s.py, s.pz, 1.0f);
+        if (p.same_grid) {
+            // For a voxel f and f - 0.5 < a < f + 0.5 (open), rint(a) = f and
+            // floor(fl(a + 0.5)) = f: the sum lies in [f, f + 1) after rounding
+            // (f is representable and a + 0.5 < f + 1 rounds to at most a
+            // value below f + 1 for |a| < 2^22).  So six comparisons with the
+            // cached interval certify both voxels unchanged.
+            if (ax > s.dvx && ax < s.fvx && ay > s.dvy && ay < s.fvy && az > s.dvz && az < s.fvz) return true;
+            const float vx = floorf(ax + 0.5f), vy = floorf(ay + 0.5f), vz = floorf(az + 0.5f);
+            const float fx = rintf(ax), fy = rintf(ay), fz = rintf(az);
+            if (!(vx >= 0.0f && vx < (float)p.dgrid.nx && vy >= 0.0f && vy < (float)p.dgrid.ny && vz >= 0.0f &&
+                  vz < (float)p.dgrid.nz))
+                return false;
+            if (!(fx >= 0.0f && fx < (float)p.fgrid.nx && fy >= 0.0f && fy < (float)p.fgrid.ny && fz >= 0.0f &&
+                  fz < (float)p.fgrid.nz))
+                return false;
+            const int64_t k = ((int64_t)(int32_t)vx * p.dgrid.ny + (int32_t)vy) * p.dgrid.nz + (int32_t)vz;
+            const uint8_t inside = __ldg(p.mask + k);
+            const int64_t fv = ((int64_t)(int32_t)fx * p.fgrid.ny + (int32_t)fy) * p.fgrid.nz + (int32_t)fz;
+            const float4* src = reinterpret_cast<const float4*>(p.field) + fv * (CPAD / 4);
+#pragma unroll
+            for (int k4 = 0; k4 < CPAD / 4; ++k4) {
+                const float4 v = __ldg(src + k4);
+                c[4 * k4] = v.x;
+                c[4 * k4 + 1] = v.y;
+                c[4 * k4 + 2] = v.z;
+                c[4 * k4 + 3] = v.w;
+            }
+            if (inside == 0) return false;
+            // a point on a voxel face (a = f + 0.5 exactly) has different
+            // domain and field voxels: leave the cache invalid
+            const bool tie = vx != fx || vy != fy || vz != fz;
+            const float nan = __int_as_float(0x7fc00000);
+            s.dvx = tie ? nan : fx - 0.5f;
+            s.dvy = tie ? nan : fy - 0.5f;
+            s.dvz = tie ? nan : fz - 0.5f;
+            s.fvx = tie ? nan : fx + 0.5f;
+            s.fvy = tie ? nan : fy + 0.5f;
+            s.fvz = tie ? nan : fz + 0.5f;
+            return true;
         }
+        const float vx = floorf(ax + 0.5f), vy = floorf(ay + 0.5f), vz = floorf(az + 0.5f);
+        const float bx = dot4(p.fgrid.row0, s.px, s.py, s.pz, 1.0f);
+        const float by = dot4(p.fgrid.row1, s.px, s.py, s.pz, 1.0f);
+        const float bz = dot4(p.fgrid.row2, s.px, s.py, s.pz, 1.0f);
         const float fx = rintf(bx), fy = rintf(by), fz = rintf(bz);
         const bool dchange = vx != s.dvx || vy != s.dvy || vz != s.dvz;
         const bool fchange = fx != s.fvx || fy != s.fvy || fz != s.fvz;
