@@ -19,6 +19,7 @@
 
 #include "tg_fmath.h"
 #include "tg_sh_table.h"
+#include "tg_sh_fold.h"
 
 #define N_DIRECTIONS 1000
 #define SOFTMAX_SCALE 100.0f
@@ -178,12 +179,27 @@ static float horner_u(const float* a, int n, float u)
     return h;
 }
 
-/* Sum of c_i Y_i, d/dtheta and (d/dphi)/sin(theta) for l <= lmax; the
- * coefficient vector c is zero-padded to the full band. */
-static model_value_t sh_raw(const float* c, int lmax, frame_t f)
+/* core.cl:111-120 */
+static float softmax(float x, float k)
+{
+    if (x * k < 30.0f) return tgm_logf(1.0f + tgm_expf(k * x)) / k;
+    return x;
+}
+
+
+/* The folded evaluation: tgsh_fold turned the coefficients of each order m
+ * and part (cos: index +m, sin: index -m) into one polynomial S(u) in
+ * u = cos^2(theta), highest power first, so that the part's sum over l is
+ * x^p S(u) with p = m & 1 and x = cos(theta).  Per block, S and S' by one
+ * Horner pass, A = x^p S and dA/dx; then the same combination into value,
+ * d/dtheta and (d/dphi)/sin(theta).  The tracking kernels run
+ * this operation sequence straight-line (tg_sh_folded.cuh). */
+static model_value_t sh_folded(const float* a, int lmax, frame_t f)
 {
     const float ct = f.ct, st = f.st, cp = f.cp, sp = f.sp;
     const float u = ct * ct;
+    const float x2 = ct + ct;
+    const float u2 = u + u;
     const float tc = cp + cp;
     float cm[TG_SH_LMAX + 1], sm[TG_SH_LMAX + 1], stp[TG_SH_LMAX + 2];
     cm[0] = 1.0f; sm[0] = 0.0f;
@@ -196,62 +212,79 @@ static model_value_t sh_raw(const float* c, int lmax, frame_t f)
     for (int k = 1; k <= lmax + 1; ++k) stp[k] = stp[k - 1] * st;
 
     model_value_t r = {0.0f, 0.0f, 0.0f};
+    int off = 0;
     for (int m = 0; m <= lmax; ++m) {
-        float A = 0.0f, B = 0.0f, Ap = 0.0f, Bp = 0.0f;
-        int any = 0;
-        for (int k = 0; k < TG_SH_NPAIRS; ++k) {
-            const int* e = TG_SH_PAIRS[k];
-            const int l = e[0];
-            if (e[1] != m || l > lmax) continue;
-            any = 1;
-            const int ip = l * (l + 1) / 2 + m;
-            const int im = l * (l + 1) / 2 - m;
-            float R = horner_u(TG_SH_COEF + e[3], e[4], u);
-            if (e[2]) R = R * ct;
-            A = fmaf(c[ip], R, A);
-            if (m > 0) B = fmaf(c[im], R, B);
-            if (l > m) {
-                float Rp = horner_u(TG_SH_COEF + e[5], e[6], u);
-                if (!e[2]) Rp = Rp * ct;
-                Ap = fmaf(c[ip], Rp, Ap);
-                if (m > 0) Bp = fmaf(c[im], Rp, Bp);
+        const int parity = m & 1;
+        const int K = (lmax - m - parity) / 2 + 1;     /* even l in [m, lmax] */
+        float X[2] = {0.0f, 0.0f}, Xp[2] = {0.0f, 0.0f};
+        int deriv = 0;
+        for (int part = 0; part < (m == 0 ? 1 : 2); ++part) {
+            const float* blk = a + off;
+            off += K;
+            float S, D = 0.0f;
+            if (K == 1) {
+                S = blk[0];
+            } else {
+                D = blk[0];
+                S = fmaf(blk[0], u, blk[1]);
+                for (int t = 2; t < K; ++t) {
+                    D = fmaf(D, u, S);
+                    S = fmaf(S, u, blk[t]);
+                }
+            }
+            if (parity) {
+                X[part] = S * ct;
+                Xp[part] = K == 1 ? S : fmaf(u2, D, S);
+                deriv = 1;
+            } else {
+                X[part] = S;
+                if (K > 1) {
+                    Xp[part] = x2 * D;
+                    deriv = 1;
+                }
             }
         }
-        if (!any) continue;
+        const float A = X[0], Ap = Xp[0], B = X[1], Bp = Xp[1];
         if (m == 0) {
             r.value = r.value + A;
-            r.dtheta = fmaf(-stp[1], Ap, r.dtheta);
+            if (deriv) r.dtheta = fmaf(-stp[1], Ap, r.dtheta);
         } else {
             const float F = fmaf(B, sm[m], A * cm[m]);
-            const float Fp = fmaf(Bp, sm[m], Ap * cm[m]);
             const float G = fmaf(-A, sm[m], B * cm[m]);
             r.value = fmaf(stp[m], F, r.value);
             const float mw = (float)m * stp[m - 1];
             const float wct = mw * ct;
             r.dtheta = fmaf(wct, F, r.dtheta);
-            r.dtheta = fmaf(-stp[m + 1], Fp, r.dtheta);
+            if (deriv) {
+                const float Fp = fmaf(Bp, sm[m], Ap * cm[m]);
+                r.dtheta = fmaf(-stp[m + 1], Fp, r.dtheta);
+            }
             r.dphi = fmaf(mw, G, r.dphi);
         }
     }
     return r;
 }
 
-/* core.cl:111-120 */
-static float softmax(float x, float k)
+/* The coefficients the tracking loop evaluates (tg_field_create does the same
+ * per voxel on the device): SH coefficients zero-padded to the full band of
+ * lmax_for(n_params) and folded (tgsh_fold), tensor coefficients as given. */
+static void model_coefficients(int32_t model, const float* params, uint32_t n_params, float* out)
 {
-    if (x * k < 30.0f) return tgm_logf(1.0f + tgm_expf(k * x)) / k;
-    return x;
-}
-
-
-/* local.py:91-120 */
-static model_value_t sh_model(const float* params, uint32_t n_params, frame_t f)
-{
+    if (model == TGO_MODEL_DTI) {
+        for (int i = 0; i < 6; ++i) out[i] = params[i];
+        return;
+    }
     float c[48];
     const int lmax = lmax_for(n_params);
     const int full = (lmax + 1) * (lmax + 2) / 2;
     for (int i = 0; i < full; ++i) c[i] = (uint32_t)i < n_params ? params[i] : 0.0f;
-    model_value_t r = sh_raw(c, lmax, f);
+    tgsh_fold(lmax, c, out);
+}
+
+/* local.py:91-120 from folded coefficients */
+static model_value_t sh_model(const float* folded, uint32_t n_params, frame_t f)
+{
+    model_value_t r = sh_folded(folded, lmax_for(n_params), f);
     /* core.cl:111-120 softmax and dsoftmax from one exponential */
     float d;
     tgm_softplus(r.value, SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &r.value, &d);
@@ -274,6 +307,7 @@ static model_value_t dti_model(const float* m, float x, float y, float z, frame_
     return r;
 }
 
+/* params: model coefficients (model_coefficients) */
 static model_value_t model_eval(int32_t model, const float* params, uint32_t n_params,
                                 float x, float y, float z, frame_t f)
 {
@@ -302,6 +336,23 @@ static void exps2(float o[3], const float t[3])      /* core.cl:101-109 */
     o[2] = fmaf(t[2], k, c * o[2]);
 }
 
+/* The folded coefficients of the field voxel a tracking loop evaluated last
+ * (folded again only when the voxel changes). */
+typedef struct {
+    const float* src;
+    float a[48];
+} voxel_fold_t;
+
+static const float* fold_voxel(const tgo_problem* p, voxel_fold_t* cache, const float* c, uint32_t C)
+{
+    if (cache->src != c) {
+        model_coefficients(p->model, c, C, cache->a);
+        cache->src = c;
+    }
+    return cache->a;
+}
+
+/* params: model coefficients (model_coefficients) */
 static void update_orientation(const tgo_problem* p, const float* params, uint32_t n_params,
                                float o[3], rng_t* rng)
 {
@@ -632,6 +683,7 @@ static uint32_t track_one(const tgo_problem* p, const float* seed, uint32_t gid,
     float time = 0.0f;
     float last[3] = {pos[0], pos[1], pos[2]};
     int first = 1;
+    voxel_fold_t fold = {NULL, {0.0f}};
     while (n < n_steps) {
         if (p->mesh) {
             /* closed surface: the seed must be inside, each later point is
@@ -652,7 +704,7 @@ static uint32_t track_one(const tgo_problem* p, const float* seed, uint32_t gid,
         }
         const float* c = field_voxel(p, pos[0], pos[1], pos[2]);
         if (!c) break;
-        update_orientation(p, c, C, o, &rng);
+        update_orientation(p, fold_voxel(p, &fold, c, C), C, o, &rng);
         *steps += 1;
         pos[0] = fmaf(p->step_size, o[0], pos[0]);
         pos[1] = fmaf(p->step_size, o[1], pos[1]);
@@ -695,6 +747,7 @@ void tgo_tod(const tgo_problem* p, const float* vertices, const uint32_t* triang
         float o[3] = {seed[4], seed[5], seed[6]};
         float last[3] = {pos[0], pos[1], pos[2]};
         int first = 1;
+    voxel_fold_t fold = {NULL, {0.0f}};
         float acc[45];
         int32_t prev[3] = {-1, -1, -1};
         for (uint32_t step = 0; step < n_steps; ++step) {
@@ -738,7 +791,7 @@ void tgo_tod(const tgo_problem* p, const float* vertices, const uint32_t* triang
                 tod_flush(coefficients, acc, prev, out_dims);
                 prev[0] = prev[1] = prev[2] = -1;
             }
-            update_orientation(p, c, C, o, &rng);
+            update_orientation(p, fold_voxel(p, &fold, c, C), C, o, &rng);
             const float len = sqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
             if (!(isfinite(o[0]) && isfinite(o[1]) && isfinite(o[2])) || len < 0.5f) break;
             pos[0] = fmaf(p->step_size, o[0], pos[0]);
@@ -772,6 +825,7 @@ void tgo_connectome(const tgo_problem* p, const tgo_bvh* boundary, const float* 
         float prev[3] = {pos[0], pos[1], pos[2]};
         float last[3] = {pos[0], pos[1], pos[2]};
         int first = 1;
+    voxel_fold_t fold = {NULL, {0.0f}};
         uint32_t tracked = 0;
         for (uint32_t step = 0; step < n_steps; ++step) {
             if (p->mesh) {
@@ -791,7 +845,7 @@ void tgo_connectome(const tgo_problem* p, const tgo_bvh* boundary, const float* 
             }
             const float* c = field_voxel(p, pos[0], pos[1], pos[2]);
             if (!c) break;
-            update_orientation(p, c, C, o, &rng);
+            update_orientation(p, fold_voxel(p, &fold, c, C), C, o, &rng);
             const float len = sqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
             if (!(isfinite(o[0]) && isfinite(o[1]) && isfinite(o[2])) || len < 0.5f) break;
             prev[0] = pos[0];
@@ -877,7 +931,9 @@ void tgo_local_evaluate(int32_t model, uint32_t n_params, const float* params,
     for (uint32_t i = 0; i < n; ++i) {
         const float* o = orientations + 4 * (size_t)i;
         const frame_t f = frame_of(o[0], o[1], o[2]);
-        const model_value_t r = model_eval(model, params + (size_t)i * n_params, n_params, o[0], o[1], o[2], f);
+        float coeffs[48];
+        model_coefficients(model, params + (size_t)i * n_params, n_params, coeffs);
+        const model_value_t r = model_eval(model, coeffs, n_params, o[0], o[1], o[2], f);
         out[3 * i] = r.value;
         out[3 * i + 1] = r.dtheta;
         out[3 * i + 2] = r.dphi;
@@ -893,7 +949,9 @@ void tgo_update_orientation(const tgo_problem* p, uint32_t n_params, const float
         rng.index = p->seed_offset + i;
         rng.step = 0u;
         float o[3] = {orientations[4 * i], orientations[4 * i + 1], orientations[4 * i + 2]};
-        update_orientation(p, params + (size_t)i * n_params, n_params, o, &rng);
+        float coeffs[48];
+        model_coefficients(p->model, params + (size_t)i * n_params, n_params, coeffs);
+        update_orientation(p, coeffs, n_params, o, &rng);
         out[4 * i] = o[0]; out[4 * i + 1] = o[1]; out[4 * i + 2] = o[2]; out[4 * i + 3] = 0.0f;
     }
 }
@@ -918,7 +976,7 @@ static void fibonacci(uint32_t n, uint32_t n_points, float d[3])
 }
 
 /* Real SH basis Y_i (i < (lmax+1)(lmax+2)/2) at one direction, the
- * value-only companion of sh_raw: Y = R * st^m * trig(m phi). */
+ * value-only basis: Y = R * st^m * trig(m phi). */
 static void sh_basis(int lmax, frame_t f, float* Y)
 {
     const float ct = f.ct, st = f.st, cp = f.cp, sp = f.sp;

@@ -188,6 +188,48 @@ __global__ void field_evaluate_kernel(Grid g, const float* __restrict__ field, u
     for (uint32_t j = 0; j < C; ++j) out[(size_t)i * C + j] = k >= 0 ? field[k * cpad + j] : 0.0f;
 }
 
+// The coefficients model_eval takes: SH coefficients folded (tgsh_fold),
+// tensor coefficients as they are.
+template <int MODEL, int LMAX, int CP>
+__device__ __forceinline__ void model_coefficients(const float (&raw)[CP], float (&c)[CP])
+{
+    if constexpr (MODEL == kModelDTI) {
+#pragma unroll
+        for (int k = 0; k < CP; ++k) c[k] = raw[k];
+    } else {
+        tgsh_fold(LMAX, raw, c);
+    }
+}
+
+// Folds a field's SH coefficients per voxel (cpad floats each, zero beyond
+// the band) for the tracking kernels.
+__global__ void fold_field_kernel(const float* __restrict__ raw, float* __restrict__ folded, uint64_t n_voxels,
+                                  uint32_t cpad, int lmax)
+{
+    const int n = (lmax + 1) * (lmax + 2) / 2;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n_voxels;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        float c[48], a[48];
+        for (uint32_t k = 0; k < cpad; ++k) c[k] = raw[v * cpad + k];
+        tgsh_fold(lmax, c, a);
+        for (uint32_t k = 0; k < cpad; ++k) folded[v * cpad + k] = (int)k < n ? a[k] : 0.0f;
+    }
+}
+
+cudaError_t launch_fold_field(const float* raw, float* folded, uint64_t n_voxels, uint32_t cpad, int lmax,
+                              cudaStream_t stream)
+{
+    if (n_voxels == 0) return cudaSuccess;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int block = 128;
+    uint64_t grid = (n_voxels + block - 1) / block;
+    if (grid > (uint64_t)sms * 32) grid = (uint64_t)sms * 32;
+    fold_field_kernel<<<(int)grid, block, 0, stream>>>(raw, folded, n_voxels, cpad, lmax);
+    return cudaGetLastError();
+}
+
 template <int MODEL, int LMAX>
 __global__ void local_evaluate_kernel(const float* __restrict__ params, uint32_t n_params,
                                       const float4* __restrict__ o, uint32_t n, float* __restrict__ out)
@@ -195,9 +237,10 @@ __global__ void local_evaluate_kernel(const float* __restrict__ params, uint32_t
     constexpr int CP = MODEL == kModelDTI ? 6 : n_coef_full(LMAX);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    float c[CP];
+    float raw[CP], c[CP];
 #pragma unroll
-    for (int k = 0; k < CP; ++k) c[k] = (uint32_t)k < n_params ? params[(size_t)i * n_params + k] : 0.0f;
+    for (int k = 0; k < CP; ++k) raw[k] = (uint32_t)k < n_params ? params[(size_t)i * n_params + k] : 0.0f;
+    model_coefficients<MODEL, LMAX, CP>(raw, c);
     const float4 v = o[i];
     const Frame f = frame_of(v.x, v.y, v.z);
     const ModelValue r = model_eval<MODEL, LMAX>(c, v.x, v.y, v.z, f);
@@ -214,9 +257,10 @@ __global__ void update_orientation_kernel(AlgoParams a, uint32_t rng_seed, uint6
     constexpr int CP = MODEL == kModelDTI ? 6 : n_coef_full(LMAX);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    float c[CP];
+    float raw[CP], c[CP];
 #pragma unroll
-    for (int k = 0; k < CP; ++k) c[k] = (uint32_t)k < n_params ? params[(size_t)i * n_params + k] : 0.0f;
+    for (int k = 0; k < CP; ++k) raw[k] = (uint32_t)k < n_params ? params[(size_t)i * n_params + k] : 0.0f;
+    model_coefficients<MODEL, LMAX, CP>(raw, c);
     RngState rng;
     rng.mwc = rng_init(rng_seed, i);
     rng.index = seed_offset + i;

@@ -237,7 +237,7 @@ int make_track_params(const tg_algorithm* a, const tg_domain* d, const tg_field*
     std::memset(&p, 0, sizeof p);
     p.domain_kind = d->d.kind;
     p.fgrid = grid_of(f->d.inv_affine, f->d.nx, f->d.ny, f->d.nz);
-    p.field = f->d.data;
+    p.field = f->d.folded;
     p.cpad = f->d.cpad;
     if (d->d.kind == kDomainMesh) {
         p.mesh = d->d.mesh;
@@ -348,8 +348,16 @@ int tg_field_create(int32_t model, const float* values, uint32_t nx, uint32_t ny
     if (e == cudaSuccess)
         e = cudaMemcpy2DAsync(f->d.data, f->d.cpad * sizeof(float), values, n_parameters * sizeof(float),
                               n_parameters * sizeof(float), nvox, cudaMemcpyHostToDevice, s);
+    // the trackers' copy: SH coefficients folded per voxel, tensors as given
+    if (e == cudaSuccess && model == TG_MODEL_SH) {
+        e = cudaMalloc(reinterpret_cast<void**>(&f->d.folded), f->d.bytes);
+        if (e == cudaSuccess) e = launch_fold_field(f->d.data, f->d.folded, nvox, f->d.cpad, f->d.lmax, s);
+    } else if (e == cudaSuccess) {
+        f->d.folded = f->d.data;
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
+        if (f->d.folded && f->d.folded != f->d.data) cudaFree(f->d.folded);
         if (f->d.data) cudaFree(f->d.data);
         delete f;
         return fail_cuda(e, "tg_field_create");
@@ -361,6 +369,7 @@ int tg_field_create(int32_t model, const float* values, uint32_t nx, uint32_t ny
 int tg_field_destroy(tg_field* field)
 {
     if (field == nullptr) return TG_OK;
+    if (field->d.folded && field->d.folded != field->d.data) cudaFree(field->d.folded);
     if (field->d.data) cudaFree(field->d.data);
     delete field;
     return TG_OK;

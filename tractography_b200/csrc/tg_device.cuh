@@ -33,10 +33,15 @@ __device__ __forceinline__ void sh_eval(const float* c, float ct, float st, floa
                                         float* val, float* dth, float* dph);
 template <int LMAX>
 __device__ __forceinline__ void sh_basis(float ct, float st, float cp, float sp, float* Y);
+template <int LMAX>
+__device__ __forceinline__ void sh_eval_folded(const float* a, float ct, float st, float cp, float sp,
+                                               float* val, float* dth, float* dph);
 
 }  // namespace tg
 
 #include "tg_sh_eval.cuh"
+#include "tg_sh_fold.h"
+#include "tg_sh_folded.cuh"
 
 namespace tg {
 
@@ -180,12 +185,14 @@ __device__ __forceinline__ float softmax(float x, float k)
     return x;
 }
 
+// local.py:91-120 from folded coefficients (tgsh_fold): the field the
+// trackers read is folded once per voxel when it is created.
 template <int LMAX>
-__device__ __forceinline__ ModelValue sh_model(const float* c, const Frame& f)
+__device__ __forceinline__ ModelValue sh_model(const float* folded, const Frame& f)
 {
     ModelValue r;
     float raw, d;
-    sh_eval<LMAX>(c, f.ct, f.st, f.cp, f.sp, &raw, &r.dtheta, &r.dphi);
+    sh_eval_folded<LMAX>(folded, f.ct, f.st, f.cp, f.sp, &raw, &r.dtheta, &r.dphi);
     // local.py:106-118: softplus of the value, derivatives times its slope
     tgm_softplus(raw, kSoftmaxScale, kSoftmaxInvScale, &r.value, &d);
     r.dtheta = r.dtheta * d;

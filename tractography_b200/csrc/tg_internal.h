@@ -25,6 +25,9 @@ constexpr int kChunkPoints = 32;   // points per output chunk (chunk = 32 x 12 B
 // (cpad = round_up(full band, 4)) so a voxel loads as float4s.
 struct FieldDev {
     float* data = nullptr;
+    // what the trackers read: SH coefficients folded per voxel (tgsh_fold,
+    // same layout and padding); the raw coefficients for tensors
+    float* folded = nullptr;
     uint32_t nx = 0, ny = 0, nz = 0;
     uint32_t n_params = 0;     // C as given by the caller
     uint32_t cpad = 0;
@@ -252,6 +255,9 @@ cudaError_t launch_gather(const float* pool, const int32_t* chunk_next, const in
 // Unit hooks (tg_aux.cu).
 cudaError_t launch_contains(const DomainDev& d, const float4* points, uint32_t n, uint8_t* out,
                             cudaStream_t stream);
+// SH fields: the folded copy the trackers read (tgsh_fold per voxel).
+cudaError_t launch_fold_field(const float* raw, float* folded, uint64_t n_voxels, uint32_t cpad, int lmax,
+                              cudaStream_t stream);
 cudaError_t launch_field_evaluate(const FieldDev& f, const float4* points, uint32_t n, float* out,
                                   cudaStream_t stream);
 cudaError_t launch_local_evaluate(int model, uint32_t n_params, const float* params,
