@@ -21,7 +21,8 @@ boundary-seeding, TOD and connectome parity tests.
 Nothing from the reference is copied into this repository: the sources are
 read from the reference tree at build time.
 
-Usage: python oracle/build_ref.py [--reference /root/reference]
+Usage: python oracle/build_ref.py [--reference DIR]   (default: $TG_REFERENCE_ROOT,
+       else the reference checkout this recipe is set up for)
 """
 
 from __future__ import annotations
@@ -37,6 +38,13 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
+
+
+def reference_root() -> Path:
+    """Where the reference sources are read from: $TG_REFERENCE_ROOT, else the
+    checkout location of this build machine.  The recipes that read the
+    reference (this one, tests/golden/make_*.py, oracle/step_error.py) share it."""
+    return Path(os.environ.get("TG_REFERENCE_ROOT", "/root/reference"))
 N_STEPS_SENTINEL = 987654
 NNZ_SENTINEL = 54321     # nonzero voxels of the FOD the seeding kernel is captured with
 
@@ -409,7 +417,7 @@ def bvh_source(kernel_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=str(reference_root()))
     args = ap.parse_args()
     reference = Path(args.reference)
     sys.path.insert(0, str(HERE.parent))

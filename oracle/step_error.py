@@ -2,7 +2,7 @@
 """Per-step error of the binary32 path against the reference's FP64 NumPy oracle.
 
 Test infrastructure only; run where the reference sources are available
-(default /root/reference).  For each workload configuration, orientation
+(see oracle.build_ref.reference_root).  For each workload configuration, orientation
 updates are drawn at random voxels of that configuration's synthetic field
 with uniformly random orientations, and one orientation update is computed
 
@@ -17,7 +17,7 @@ updated unit orientation, i.e. radians for small errors; a 0.1-voxel step
 turns it into a position error of step_size x error.  Writes the table to
 profiles/step_error_fp64.md.
 
-Usage: python oracle/step_error.py [--reference /root/reference] [--samples 20000]
+Usage: python oracle/step_error.py [--reference DIR] [--samples 20000]
 """
 
 from __future__ import annotations
@@ -30,6 +30,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parent))
+from oracle.build_ref import reference_root  # noqa: E402
 
 
 def sample(field_values, rng, n):
@@ -44,7 +45,7 @@ def sample(field_values, rng, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=str(reference_root()))
     ap.add_argument("--samples", type=int, default=20000)
     args = ap.parse_args()
     from oracle.refstubs import install_stubs

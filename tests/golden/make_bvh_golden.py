@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Golden vectors for the boundary BVH, from the reference itself.
 
-Run where the reference sources are available (default /root/reference)
+Run where the reference sources are available (oracle.build_ref.reference_root)
 after ``python oracle/build_ref.py``; writes tests/golden/bvh_reference.npz.
 
 Three triangle sets:
@@ -41,6 +41,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 
+from oracle.build_ref import reference_root  # noqa: E402
 from oracle.refstubs import install_stubs  # noqa: E402
 
 
@@ -72,7 +73,7 @@ def segments(rng, vertices, faces, scale):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=str(reference_root()))
     args = ap.parse_args()
     install_stubs(Path(args.reference))
     import tractography as ref  # noqa: E402  (the reference package)

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Generate golden vectors from the reference's own NumPy implementations.
 
-Run on a machine where the reference sources are available (default
-/root/reference); writes tests/golden/reference_numpy.npz.  The reference
+Run on a machine where the reference sources are available
+(oracle.build_ref.reference_root); writes tests/golden/reference_numpy.npz.  The reference
 imports pyopencl, nibabel, trimesh and nimesh at module level; none of their
 functionality is used by the functions called here, so minimal stand-ins are
 registered in sys.modules first (pyopencl.cltypes dtypes, nibabel's
@@ -24,6 +24,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 
+from oracle.build_ref import reference_root  # noqa: E402
 from oracle.refstubs import install_stubs  # noqa: E402
 
 
@@ -44,7 +45,7 @@ def quadratic_fod(tg, base, eps, C):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=str(reference_root()))
     args = ap.parse_args()
     install_stubs(Path(args.reference))
     import tractography as ref  # noqa: E402  (the reference package)
