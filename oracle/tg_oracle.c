@@ -79,7 +79,8 @@ static float randn(uint32_t s[2])                    /* core.cl:240-245 */
     float n = randu(s);
     while (n <= 0.0f) n = randu(s);
     const float radius = sqrtf(-2.0f * tgm_logf(n));
-    return radius * tgm_cosf(TGM_TWO_PI * randu(s));
+    /* cos(2 pi randu): the same draw, as its 24-bit integer */
+    return radius * tgm_cos2pi_u24(mwc64x(s) >> 8);
 }
 
 /* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter-based stream
@@ -137,15 +138,19 @@ static frame_t frame_of(float x, float y, float z)
         f.ct = 1.0f; f.st = 0.0f; f.cp = 1.0f; f.sp = 0.0f;
         return f;
     }
-    const float ir = 1.0f / r;
-    f.ct = fminf(fmaxf(z * ir, -1.0f), 1.0f);        /* core.cl:151 clamp */
+    /* off the axis, 1/r = rho q and 1/rho = r q with q = 1/(r rho) */
     const float rho = sqrtf(rho2);
-    f.st = fminf(rho * ir, 1.0f);
-    if (rho > 0.0f) {
-        const float irho = 1.0f / rho;
+    const float rr = r * rho;
+    if (rr > 0.0f) {
+        const float q = 1.0f / rr;
+        const float ir = rho * q, irho = r * q;
+        f.ct = fminf(fmaxf(z * ir, -1.0f), 1.0f);    /* core.cl:151 clamp */
+        f.st = fminf(rho * ir, 1.0f);
         f.cp = x * irho;
         f.sp = y * irho;
     } else {                                         /* atan2(0, 0) = 0 */
+        f.ct = fminf(fmaxf(z / r, -1.0f), 1.0f);
+        f.st = 0.0f;
         f.cp = 1.0f;
         f.sp = 0.0f;
     }
@@ -163,7 +168,9 @@ static float dot4(const float* a, float x, float y, float z, float w)
 /* Local models                                                        */
 /* ------------------------------------------------------------------ */
 
-typedef struct { float value, dtheta, dphi; } model_value_t;
+/* value, d/dtheta, (d/dphi)/sin(theta), and 1 / max(value, 1e-6) (the
+ * drift's divisor, algorithm.py:98, :216) */
+typedef struct { float value, dtheta, dphi, inv; } model_value_t;
 
 static int lmax_for(uint32_t n_params)
 {
@@ -211,7 +218,7 @@ static model_value_t sh_folded(const float* a, int lmax, frame_t f)
     stp[0] = 1.0f;
     for (int k = 1; k <= lmax + 1; ++k) stp[k] = stp[k - 1] * st;
 
-    model_value_t r = {0.0f, 0.0f, 0.0f};
+    model_value_t r = {0.0f, 0.0f, 0.0f, 0.0f};
     int off = 0;
     for (int m = 0; m <= lmax; ++m) {
         const int parity = m & 1;
@@ -287,7 +294,7 @@ static model_value_t sh_model(const float* folded, uint32_t n_params, frame_t f)
     model_value_t r = sh_folded(folded, lmax_for(n_params), f);
     /* core.cl:111-120 softmax and dsoftmax from one exponential */
     float d;
-    tgm_softplus(r.value, SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &r.value, &d);
+    tgm_softplus(r.value, SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &r.value, &d, &r.inv);
     r.dtheta = r.dtheta * d;
     r.dphi = r.dphi * d;
     return r;
@@ -304,6 +311,7 @@ static model_value_t dti_model(const float* m, float x, float y, float z, frame_
     const float etx = f.ct * f.cp, ety = f.ct * f.sp, etz = -f.st;
     r.dtheta = 2.0f * fmaf(duz, etz, fmaf(duy, ety, dux * etx));
     r.dphi = 2.0f * fmaf(duy, f.cp, dux * (-f.sp));
+    r.inv = 1.0f / cl_maxf(r.value, 1e-6f);
     return r;
 }
 
@@ -360,7 +368,7 @@ static void update_orientation(const tgo_problem* p, const float* params, uint32
     const model_value_t mv = model_eval(p->model, params, n_params, o[0], o[1], o[2], f);
     const float etx = f.ct * f.cp, ety = f.ct * f.sp, etz = -f.st;
     const float epx = -f.sp, epy = f.cp;
-    const float inv = 1.0f / cl_maxf(mv.value, 1e-6f);
+    const float inv = mv.inv;
     const float gx = fmaf(mv.dphi, epx, mv.dtheta * etx);
     const float gy = fmaf(mv.dphi, epy, mv.dtheta * ety);
     const float gz = mv.dtheta * etz;
@@ -1106,8 +1114,10 @@ void tgo_math(int which, const float* x, uint32_t n, float* out)
         case 3: out[i] = tgm_logf(x[i]); break;
         case 4: { float c, k; tgm_exps2_factors(x[i], &c, &k); out[i] = c; } break;
         case 5: { float c, k; tgm_exps2_factors(x[i], &c, &k); out[i] = k; } break;
-        case 6: { float v, d; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d); out[i] = v; } break;
-        case 7: { float v, d; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d); out[i] = d; } break;
+        case 6: { float v, d, q; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d, &q); out[i] = v; } break;
+        case 7: { float v, d, q; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d, &q); out[i] = d; } break;
+        case 8: { float v, d, q; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d, &q); out[i] = q; } break;
+        case 9: out[i] = tgm_cos2pi_u24((uint32_t)x[i]); break;
         default: out[i] = x[i]; break;
         }
     }

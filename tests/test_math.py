@@ -68,6 +68,21 @@ def test_softplus_and_slope(oracle):
     assert np.abs(slope - want_slope).max() <= 4 * np.spacing(np.float32(1.0))
     assert np.all(slope[100 * x >= 30] == 1.0)
     assert np.isnan(oracle.math("softplus_slope", np.array([np.nan], np.float32))[0])
+    # the drift's divisor 1 / max(softplus, 1e-6) shares the slope's division
+    inv = oracle.math("softplus_inv_floor", x).astype(np.float64)
+    want_inv = 1 / np.maximum(got, 1e-6)
+    assert np.all(np.abs(inv - want_inv) <= 3 * np.spacing(want_inv.astype(np.float32)))
+
+
+def test_cos2pi_of_24_bit_draws(oracle):
+    """cos(2 pi k 2^-24) with exact integer quarter turns (Box-Muller's angle,
+    core.cl:240-245): within 2 ulp of float64, or 2^-24 absolute near its zeros."""
+    k = np.concatenate([np.arange(0, 1 << 24, 37, dtype=np.int64),
+                        np.array([0, 1, (1 << 21) - 1, 1 << 21, (1 << 22), (1 << 24) - 1], np.int64)])
+    got = oracle.math("cos2pi_u24", k.astype(np.float32)).astype(np.float64)
+    want = np.cos(2 * np.pi * k.astype(np.float64) / 2.0 ** 24)
+    err = np.abs(got - want)
+    assert np.all(err <= np.maximum(2 * np.spacing(np.abs(want).astype(np.float32)), 2.0 ** -24))
 
 
 def test_log_within_two_ulp(oracle):

@@ -105,7 +105,8 @@ __device__ __forceinline__ float randn(Mwc& s)
     float n = randu(s);
     while (n <= 0.0f) n = randu(s);   // terminates: 2^-24 resolution, MWC64X period ~2^63
     const float radius = sqrtf(-2.0f * tgm_logf(n));
-    return radius * tgm_cosf(TGM_TWO_PI * randu(s));
+    // cos(2 pi randu): the same draw, as its 24-bit integer
+    return radius * tgm_cos2pi_u24(mwc64x(s) >> 8);
 }
 
 __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
@@ -141,7 +142,10 @@ struct Frame {
     float ct, st, cp, sp;
 };
 
-// cart2sph (core.cl:142-153) as direction cosines of colatitude/azimuth.
+// cart2sph (core.cl:142-153) as direction cosines of colatitude/azimuth:
+// ct = z/r, st = rho/r, cp = x/rho, sp = y/rho.  Off the axis both
+// reciprocals come from one division, 1/r = rho q and 1/rho = r q with
+// q = 1/(r rho); on it (r rho rounds to 0) phi is taken as 0.
 __device__ __forceinline__ Frame frame_of(float x, float y, float z)
 {
     Frame f;
@@ -152,15 +156,18 @@ __device__ __forceinline__ Frame frame_of(float x, float y, float z)
         f.ct = 1.0f; f.st = 0.0f; f.cp = 1.0f; f.sp = 0.0f;
         return f;
     }
-    const float ir = 1.0f / r;
-    f.ct = fminf(fmaxf(z * ir, -1.0f), 1.0f);
     const float rho = sqrtf(rho2);
-    f.st = fminf(rho * ir, 1.0f);
-    if (rho > 0.0f) {
-        const float irho = 1.0f / rho;
+    const float rr = r * rho;
+    if (rr > 0.0f) {
+        const float q = 1.0f / rr;
+        const float ir = rho * q, irho = r * q;
+        f.ct = fminf(fmaxf(z * ir, -1.0f), 1.0f);
+        f.st = fminf(rho * ir, 1.0f);
         f.cp = x * irho;
         f.sp = y * irho;
     } else {
+        f.ct = fminf(fmaxf(z / r, -1.0f), 1.0f);
+        f.st = 0.0f;
         f.cp = 1.0f;
         f.sp = 0.0f;
     }
@@ -176,6 +183,7 @@ __device__ __forceinline__ float dot4(float4 a, float x, float y, float z, float
 
 struct ModelValue {
     float value, dtheta, dphi;
+    float inv;   // 1 / max(value, 1e-6), the drift's divisor (algorithm.py:98, :216)
 };
 
 // core.cl:111-115 (the seeding kernel's model value; tracking uses tgm_softplus)
@@ -194,7 +202,7 @@ __device__ __forceinline__ ModelValue sh_model(const float* folded, const Frame&
     float raw, d;
     sh_eval_folded<LMAX>(folded, f.ct, f.st, f.cp, f.sp, &raw, &r.dtheta, &r.dphi);
     // local.py:106-118: softplus of the value, derivatives times its slope
-    tgm_softplus(raw, kSoftmaxScale, kSoftmaxInvScale, &r.value, &d);
+    tgm_softplus(raw, kSoftmaxScale, kSoftmaxInvScale, &r.value, &d, &r.inv);
     r.dtheta = r.dtheta * d;
     r.dphi = r.dphi * d;
     return r;
@@ -210,6 +218,7 @@ __device__ __forceinline__ ModelValue dti_model(const float* m, float x, float y
     const float etx = f.ct * f.cp, ety = f.ct * f.sp, etz = -f.st;
     r.dtheta = 2.0f * fmaf(duz, etz, fmaf(duy, ety, dux * etx));
     r.dphi = 2.0f * fmaf(duy, f.cp, dux * (-f.sp));
+    r.inv = 1.0f / cl_max(r.value, 1e-6f);
     return r;
 }
 
@@ -260,7 +269,7 @@ __device__ __forceinline__ void update_orientation(const AlgoParams& a, const fl
     const ModelValue mv = model_eval<MODEL, LMAX>(c, ox, oy, oz, f);
     const float etx = f.ct * f.cp, ety = f.ct * f.sp, etz = -f.st;
     const float epx = -f.sp, epy = f.cp;
-    const float inv = 1.0f / cl_max(mv.value, 1e-6f);
+    const float inv = mv.inv;
     const float gx = fmaf(mv.dphi, epx, mv.dtheta * etx);
     const float gy = fmaf(mv.dphi, epy, mv.dtheta * ety);
     const float gz = mv.dtheta * etz;

@@ -237,19 +237,59 @@ TGM_FN void tgm_exps2_factors(float n2, float* c_out, float* k_out)
  * E = e^{kx} the derivative is E / (1 + E).  For kx >= 30 the derivative
  * rounds to 1 in binary32 (e^{-30} < 2^-24), and NaN propagates.  The
  * division by k is a multiplication by inv_k = 1/k rounded.
+ *
+ * The tracking step also divides by the model value, floored at 1e-6
+ * (algorithm.py:98, :216); *inv_floor receives 1 / max(value, 1e-6).  Below
+ * kx = 30 both reciprocals come from one division,
+ * q = 1 / ((1 + E) max(value, 1e-6)).
  */
-TGM_FN void tgm_softplus(float x, float k, float inv_k, float* value, float* derivative)
+TGM_FN void tgm_softplus(float x, float k, float inv_k, float* value, float* derivative, float* inv_floor)
 {
     const float kx = x * k;
     if (kx < 30.0f) {
         const float e = tgm_expf(kx);
         const float one_e = 1.0f + e;
-        *value = tgm_logf(one_e) * inv_k;
-        *derivative = e / one_e;
+        const float v = tgm_logf(one_e) * inv_k;
+        const float m = (v < 1e-6f) ? 1e-6f : v;
+        const float q = 1.0f / (one_e * m);
+        *value = v;
+        *derivative = (e * m) * q;
+        *inv_floor = one_e * q;
     } else {
         *value = x;
         *derivative = (kx == kx) ? 1.0f : kx;
+        *inv_floor = 1.0f / ((x < 1e-6f) ? 1e-6f : x);
     }
+}
+
+/*
+ * cos(2 pi k / 2^24) for a 24-bit k (the uniform k 2^-24 of core.cl:212-214
+ * that Box-Muller turns into an angle, core.cl:240-245).  The quarter turns
+ * q = round(k / 2^22) come out exactly in integer arithmetic; the remainder
+ * |r| <= 2^21 becomes an angle |t| <= pi/4 by one multiplication, and
+ * cos(t + q pi/2) is cos t, -sin t, -cos t or sin t (series as in
+ * tgm_sincosf).  No float argument reduction is needed.
+ */
+#define TGM_TWO_PI_2M24 0x1.921fb6p-22f   /* float(2 pi) / 2^24, exact scaling */
+TGM_FN float tgm_cos2pi_u24(uint32_t k)
+{
+    const uint32_t q = (k + 0x200000u) >> 22;
+    const int32_t r = (int32_t)k - (int32_t)(q << 22);
+    const float t = (float)r * TGM_TWO_PI_2M24;
+    const float t2 = t * t;
+    float ps = 0x1.71de3ap-19f;                  /*  1/9! */
+    ps = fmaf(ps, t2, -0x1.a01a02p-13f);         /* -1/7! */
+    ps = fmaf(ps, t2, 0x1.111112p-7f);           /*  1/5! */
+    ps = fmaf(ps, t2, -0x1.555556p-3f);          /* -1/3! */
+    const float st = fmaf(t * t2, ps, t);
+    float pc = -0x1.27e4fcp-22f;                 /* -1/10! */
+    pc = fmaf(pc, t2, 0x1.a01a02p-16f);          /*  1/8!  */
+    pc = fmaf(pc, t2, -0x1.6c16c2p-10f);         /* -1/6!  */
+    pc = fmaf(pc, t2, 0x1.555556p-5f);           /*  1/4!  */
+    pc = fmaf(pc, t2, -0.5f);
+    const float ct = fmaf(t2, pc, 1.0f);
+    const float c = (q & 1u) ? st : ct;
+    return ((q + 1u) & 2u) ? -c : c;
 }
 
 #endif /* TG_FMATH_H */
