@@ -78,7 +78,7 @@ static float randn(uint32_t s[2])                    /* core.cl:240-245 */
 {
     float n = randu(s);
     while (n <= 0.0f) n = randu(s);
-    const float radius = sqrtf(-2.0f * tgm_logf(n));
+    const float radius = sqrtf(-2.0f * tgm_log_pos(n));
     /* cos(2 pi randu): the same draw, as its 24-bit integer */
     return radius * tgm_cos2pi_u24(mwc64x(s) >> 8);
 }
@@ -114,7 +114,7 @@ static void philox_normal2(uint64_t key, uint64_t index, uint32_t step, float* n
     tgo_philox(ctr, k, w);
     const float u1 = (float)((w[0] >> 8) + 1u) * 0x1p-24f;
     const float u2 = (float)(w[1] >> 8) * 0x1p-24f;
-    const float radius = sqrtf(-2.0f * tgm_logf(u1));
+    const float radius = sqrtf(-2.0f * tgm_log_pos(u1));
     float s, c;
     tgm_sincosf(TGM_TWO_PI * u2, &s, &c);
     *n1 = radius * c;
@@ -1118,6 +1118,7 @@ void tgo_math(int which, const float* x, uint32_t n, float* out)
         case 7: { float v, d, q; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d, &q); out[i] = d; } break;
         case 8: { float v, d, q; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d, &q); out[i] = q; } break;
         case 9: out[i] = tgm_cos2pi_u24((uint32_t)x[i]); break;
+        case 10: out[i] = tgm_log_pos(x[i]); break;
         default: out[i] = x[i]; break;
         }
     }

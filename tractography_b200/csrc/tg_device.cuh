@@ -104,7 +104,7 @@ __device__ __forceinline__ float randn(Mwc& s)
 {
     float n = randu(s);
     while (n <= 0.0f) n = randu(s);   // terminates: 2^-24 resolution, MWC64X period ~2^63
-    const float radius = sqrtf(-2.0f * tgm_logf(n));
+    const float radius = sqrtf(-2.0f * tgm_log_pos(n));
     // cos(2 pi randu): the same draw, as its 24-bit integer
     return radius * tgm_cos2pi_u24(mwc64x(s) >> 8);
 }
@@ -129,7 +129,7 @@ __device__ __forceinline__ void philox_normal2(uint64_t key, uint64_t index, uin
                                   make_uint2((uint32_t)key, (uint32_t)(key >> 32)));
     const float u1 = (float)((w.x >> 8) + 1u) * 0x1p-24f;
     const float u2 = (float)(w.y >> 8) * 0x1p-24f;
-    const float radius = sqrtf(-2.0f * tgm_logf(u1));
+    const float radius = sqrtf(-2.0f * tgm_log_pos(u1));
     float s, c;
     tgm_sincosf(TGM_TWO_PI * u2, &s, &c);
     *n1 = radius * c;

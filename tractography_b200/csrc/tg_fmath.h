@@ -199,6 +199,33 @@ TGM_FN float tgm_logf(float x_in)
 }
 
 /*
+ * log for positive, finite, normal x -- the tracking step's arguments:
+ * Box-Muller's uniform in [2^-24, 1) and 1 + e^{kx} in [1, 1 + e^30].
+ * Same series as tgm_logf, without its special-value and subnormal
+ * handling; the reduction x = m 2^e, m in [sqrt(1/2), sqrt(2)), comes from
+ * one integer subtraction: with B the bits of sqrt(1/2), d = bits(x) - B,
+ * m has the bits B + (d mod 2^23) (a carry out of the mantissa field lifts
+ * m into [1, sqrt(2))) and e = floor(d / 2^23).
+ */
+TGM_FN float tgm_log_pos(float x)
+{
+    const uint32_t d = tgm_f2u(x) - 0x3f3504f3u;
+    const int e = (int)((d + 0x3f800000u) >> 23) - 127;
+    const float m = tgm_u2f((d & 0x007fffffu) + 0x3f3504f3u);
+    const float f = m - 1.0f;
+    const float s = f / (2.0f + f);
+    const float z = s * s;
+    float p = 0x1.c71c72p-4f;                         /* 1/9 */
+    p = fmaf(p, z, 0x1.24924ap-3f);                   /* 1/7 */
+    p = fmaf(p, z, 0x1.99999ap-3f);                   /* 1/5 */
+    p = fmaf(p, z, 0x1.555556p-2f);                   /* 1/3 */
+    const float two_s = s + s;
+    const float logm = fmaf(two_s * z, p, two_s);
+    const float ef = (float)e;
+    return fmaf(ef, TGM_LN2_HI, fmaf(ef, TGM_LN2_LO, logm));
+}
+
+/*
  * The exponential map's factors (core.cl:101-109) from n2 = |t|^2 > 0:
  * c = cos(n) and k = sin(n) / n with n = sqrt(n2).  For n2 < 1 both are
  * Taylor series in n2 (cos to n^12, sin(n)/n to n^12 / 13!; truncation
@@ -245,21 +272,20 @@ TGM_FN void tgm_exps2_factors(float n2, float* c_out, float* k_out)
  */
 TGM_FN void tgm_softplus(float x, float k, float inv_k, float* value, float* derivative, float* inv_floor)
 {
+    /* branch-free: one exponential, one logarithm and one division whatever
+     * kx is (the exponential's argument is capped at 30, where it is not
+     * used, so that the logarithm stays in its domain) */
     const float kx = x * k;
-    if (kx < 30.0f) {
-        const float e = tgm_expf(kx);
-        const float one_e = 1.0f + e;
-        const float v = tgm_logf(one_e) * inv_k;
-        const float m = (v < 1e-6f) ? 1e-6f : v;
-        const float q = 1.0f / (one_e * m);
-        *value = v;
-        *derivative = (e * m) * q;
-        *inv_floor = one_e * q;
-    } else {
-        *value = x;
-        *derivative = (kx == kx) ? 1.0f : kx;
-        *inv_floor = 1.0f / ((x < 1e-6f) ? 1e-6f : x);
-    }
+    const int small = kx < 30.0f;
+    const float e = tgm_expf(fminf(kx, 30.0f));
+    const float one_e = 1.0f + e;
+    const float lg = tgm_log_pos(one_e) * inv_k;
+    const float v = small ? lg : x;
+    const float m = (v < 1e-6f) ? 1e-6f : v;
+    const float q = 1.0f / (small ? one_e * m : m);
+    *value = v;
+    *derivative = small ? (e * m) * q : ((kx == kx) ? 1.0f : kx);
+    *inv_floor = small ? one_e * q : q;
 }
 
 /*
