@@ -133,6 +133,21 @@ static frame_t frame_of(float x, float y, float z)
     frame_t f;
     const float rho2 = fmaf(y, y, x * x);
     const float r2 = fmaf(z, z, rho2);
+    if (fabsf(r2 - 1.0f) < 0x1p-14f) {               /* near unit: 1/r = 1.5 - r^2/2 */
+        const float ir = fmaf(-0.5f, r2, 1.5f);
+        const float rho = sqrtf(rho2);
+        f.ct = fminf(fmaxf(z * ir, -1.0f), 1.0f);
+        f.st = fminf(rho * ir, 1.0f);
+        if (rho > 0.0f) {
+            const float irho = 1.0f / rho;
+            f.cp = x * irho;
+            f.sp = y * irho;
+        } else {
+            f.cp = 1.0f;
+            f.sp = 0.0f;
+        }
+        return f;
+    }
     const float r = sqrtf(r2);
     if (r <= 0.0f) {                                 /* core.cl:144-146 */
         f.ct = 1.0f; f.st = 0.0f; f.cp = 1.0f; f.sp = 0.0f;
@@ -1119,6 +1134,7 @@ void tgo_math(int which, const float* x, uint32_t n, float* out)
         case 8: { float v, d, q; tgm_softplus(x[i], SOFTMAX_SCALE, SOFTMAX_INV_SCALE, &v, &d, &q); out[i] = q; } break;
         case 9: out[i] = tgm_cos2pi_u24((uint32_t)x[i]); break;
         case 10: out[i] = tgm_log_pos(x[i]); break;
+        case 11: out[i] = tgm_exp_upto30(x[i]); break;
         default: out[i] = x[i]; break;
         }
     }

@@ -100,6 +100,15 @@ def test_cos2pi_of_24_bit_draws(oracle):
     assert np.all(err <= np.maximum(2 * np.spacing(np.abs(want).astype(np.float32)), 2.0 ** -24))
 
 
+def test_exp_up_to_30_within_two_ulp(oracle):
+    """softplus's exponential (argument capped at 30): 2 ulp down to -87.3, then 0."""
+    x = np.linspace(-87.3, 30.0, 2_000_001, dtype=np.float32)
+    err = ulp_error(oracle.math("exp_upto30", x), np.exp(x.astype(np.float64)))
+    assert err.max() <= 2.0
+    below = oracle.math("exp_upto30", np.array([-87.34, -100.0, -np.inf], np.float32))
+    assert np.all(below == 0.0)
+
+
 def test_log_within_two_ulp(oracle):
     rng = np.random.default_rng(0)
     x = np.concatenate([

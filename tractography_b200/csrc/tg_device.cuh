@@ -143,14 +143,32 @@ struct Frame {
 };
 
 // cart2sph (core.cl:142-153) as direction cosines of colatitude/azimuth:
-// ct = z/r, st = rho/r, cp = x/rho, sp = y/rho.  Off the axis both
-// reciprocals come from one division, 1/r = rho q and 1/rho = r q with
-// q = 1/(r rho); on it (r rho rounds to 0) phi is taken as 0.
+// ct = z/r, st = rho/r, cp = x/rho, sp = y/rho.  Orientations leave the
+// exponential map with |o|^2 = 1 within a few ulp; for |r^2 - 1| < 2^-14,
+// 1/r = 1.5 - r^2/2 to within 1.4e-9 relative (its expansion about 1), far
+// inside binary32 rounding.  Otherwise both reciprocals come from one
+// division, 1/r = rho q and 1/rho = r q with q = 1/(r rho); on the axis
+// (r rho rounds to 0) phi is taken as 0.
 __device__ __forceinline__ Frame frame_of(float x, float y, float z)
 {
     Frame f;
     const float rho2 = fmaf(y, y, x * x);
     const float r2 = fmaf(z, z, rho2);
+    if (fabsf(r2 - 1.0f) < 0x1p-14f) {
+        const float ir = fmaf(-0.5f, r2, 1.5f);
+        const float rho = sqrtf(rho2);
+        f.ct = fminf(fmaxf(z * ir, -1.0f), 1.0f);
+        f.st = fminf(rho * ir, 1.0f);
+        if (rho > 0.0f) {
+            const float irho = 1.0f / rho;
+            f.cp = x * irho;
+            f.sp = y * irho;
+        } else {
+            f.cp = 1.0f;
+            f.sp = 0.0f;
+        }
+        return f;
+    }
     const float r = sqrtf(r2);
     if (r <= 0.0f) {
         f.ct = 1.0f; f.st = 0.0f; f.cp = 1.0f; f.sp = 0.0f;

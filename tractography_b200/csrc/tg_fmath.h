@@ -226,6 +226,29 @@ TGM_FN float tgm_log_pos(float x)
 }
 
 /*
+ * e^x for x <= 30, not NaN (softplus's argument, capped at 30 by its
+ * caller): the series of tgm_expf, scaled by 2^k in one step; below
+ * -87.3 (where the result would leave the normal range) the result is 0.
+ */
+TGM_FN float tgm_exp_upto30(float x_in)
+{
+    const float x = fmaxf(x_in, -87.33654f);
+    const float k = rintf(x * TGM_LOG2E);             /* -126 <= k <= 44 */
+    float r = fmaf(-k, TGM_LN2_HI, x);
+    r = fmaf(-k, TGM_LN2_LO, r);
+    float p = 0x1.a01a02p-13f;                   /* 1/7! */
+    p = fmaf(p, r, 0x1.6c16c2p-10f);             /* 1/6! */
+    p = fmaf(p, r, 0x1.111112p-7f);              /* 1/5! */
+    p = fmaf(p, r, 0x1.555556p-5f);              /* 1/4! */
+    p = fmaf(p, r, 0x1.555556p-3f);              /* 1/3! */
+    p = fmaf(p, r, 0.5f);
+    p = fmaf(p, r, 1.0f);
+    p = fmaf(p, r, 1.0f);
+    const float result = p * tgm_pow2i((int)k);
+    return (x_in < -87.33654f) ? 0.0f : result;
+}
+
+/*
  * The exponential map's factors (core.cl:101-109) from n2 = |t|^2 > 0:
  * c = cos(n) and k = sin(n) / n with n = sqrt(n2).  For n2 < 1 both are
  * Taylor series in n2 (cos to n^12, sin(n)/n to n^12 / 13!; truncation
@@ -277,7 +300,7 @@ TGM_FN void tgm_softplus(float x, float k, float inv_k, float* value, float* der
      * used, so that the logarithm stays in its domain) */
     const float kx = x * k;
     const int small = kx < 30.0f;
-    const float e = tgm_expf(fminf(kx, 30.0f));
+    const float e = tgm_exp_upto30(fminf(kx, 30.0f));
     const float one_e = 1.0f + e;
     const float lg = tgm_log_pos(one_e) * inv_k;
     const float v = small ? lg : x;
