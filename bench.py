@@ -390,6 +390,16 @@ def run_ours(args):
         },
         "clocks": sampler.summary(),
     }
+    line["roofline"]["note"] = ("algorithmic bytes: the 184 B gather of a step; a voxel's coefficients stay in "
+                                "registers for the ~1250 steps a streamline spends in it, so DRAM carries ~0.3 B "
+                                "per step (traffic) and frac above 1 is that reuse, not DRAM; the kernel is bound "
+                                "by instruction issue (issue)")
+    inst = profile_constant("thread_inst_per_step")
+    issue = profile_constant("issue_active_pct")
+    if inst is not None and issue is not None:
+        line["issue"] = {"thread_instructions_per_step": inst, "issue_active": issue / 100.0,
+                         "source": "full-size ncu counters of the tracking kernel "
+                                   "(profiles/track_persistent_config1.md)"}
     flop = profile_constant("fp32_flop_per_step")
     if flop is not None:
         tflops = kernel_steps_per_s * flop / 1e12

@@ -832,6 +832,7 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
             TG_TRY(ensure(&t->d_totals, &t->cap_totals, 2));
             TG_TRY(launch_offsets(t->lengths, n_seeds, t->masked, t->offsets, t->d_totals, t->scan_temp, &temp_bytes,
                                   s));
+            t->launches += 2;   // masked_lengths_kernel, offsets_total_kernel (the scan between is cub's)
             unsigned long long totals[2] = {0ull, 0ull};
             TG_TRY(cudaMemcpyAsync(totals, t->d_totals, sizeof totals, cudaMemcpyDeviceToHost, s));
             TG_TRY(cudaStreamSynchronize(s));
@@ -1142,6 +1143,7 @@ int tg_tracker_run_jobs(tg_tracker* t, const tg_job* jobs, uint32_t n_jobs, int 
             TG_TRY(ensure(&t->d_totals, &t->cap_totals, 2));
             TG_TRY(launch_offsets(t->lengths, (uint32_t)n_total, t->masked, t->offsets, t->d_totals, t->scan_temp,
                                   &temp_bytes, s));
+            t->launches += 2;   // masked_lengths_kernel, offsets_total_kernel
             unsigned long long totals[2] = {0ull, 0ull};
             TG_TRY(cudaMemcpyAsync(totals, t->d_totals, sizeof totals, cudaMemcpyDeviceToHost, s));
             TG_TRY(cudaStreamSynchronize(s));
