@@ -17,16 +17,21 @@ loop that passed both the domain and the field check (tracking.py:121-147).
 
 Reported:
   value     device-resident throughput: seeds already in HBM, one
-            persistent-tracker run per batch, packed output left on the
-            device; CUDA events on the tracker's stream, max over ranks.
-  e2e       the same metric through the C ABI with host buffers: the
-            host-to-device copy of the batch's seeds, tracking, and the
-            device-to-host copy of lengths, offsets and packed points are
-            all inside the timed region.
+            persistent-tracker run per job, packed output left on the
+            device; two jobs in flight (``--in-flight``), each slot with its
+            own stream and tracker, so the next job's blocks take the SMs
+            the previous job's tail frees; CUDA events spanning every
+            stream, max over ranks.
+  single_job  the same jobs one at a time (each run returns before the
+            next starts).
+  e2e       the same metric through the C ABI with host buffers, jobs in
+            flight as for value: the host-to-device copy of the job's seeds,
+            tracking, and the device-to-host copy of lengths, offsets and
+            packed points are all inside the timed region.
   roofline  the tracking kernel's algorithmic bytes per step
             (4 C + 4 + 16 step/save_at = 184.064 B at C = 45) times the
-            steps of a launch over its event-timed duration, against the
-            measured HBM copy bandwidth.
+            steps of a launch over its event-timed duration (the
+            one-at-a-time leg), against the measured HBM copy bandwidth.
   cpu_baseline  the CPU oracle (plain-C restatement of the reference
             kernel, OpenMP over seeds) on a bounded sample of the same
             workload on this host's cores.
@@ -78,6 +83,9 @@ def parse_args():
     p.add_argument("--seeds", type=int, default=1000000, help="seeds per step (one tg.tractogram job)")
     p.add_argument("--batch", type=int, default=50000, help="reference batch_size inside a job")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--in-flight", type=int, default=2,
+                   help="config1: jobs in flight (each on its own stream and tracker); the next job's blocks "
+                        "take the SMs the previous job's tail frees")
     p.add_argument("--workload", choices=["config1", "config0", "mixed", "config2", "serve", "tod", "connectome"],
                    default="config1",
                    help="config1 (default headline), the 64-job mixed workload, the DTI + mesh workload, or "
@@ -242,100 +250,144 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local_rank)
-    runtime = tg.CudaRuntime(local_rank)
-    lib = runtime.lib
     n_job = args.seeds
-    fod, field, domain, seeds, algorithm = setup_workload(rank, n_job, runtime)
     n_steps = int(math.floor(MAX_LENGTH / SAVE_AT))
+    # every streamline fits a pool of n_job x n_steps points: no retry waves,
+    # and each slot's tracker takes only its own share of the device
+    pool = n_job * n_steps
+    runtime = tg.CudaRuntime(local_rank, pool_points=pool)
+    lib = runtime.lib
+    fod, field, domain, seeds, algorithm = setup_workload(rank, n_job, runtime)
     n_batches = (n_job + args.batch - 1) // args.batch
     # one reference RNG seed per batch, drawn in batch order for every job
     rng_seeds = [np.array([algorithm.get_rng_seed() for _ in range(n_batches)], dtype=np.uint32)
                  for _ in range(args.warmup + args.steps)]
-    stream = runtime.stream
-    sh = ctypes.c_void_p(runtime.stream_handle)
+    in_flight = max(1, args.in_flight)
     with runtime.device_scope():
         d_handle = domain.device(runtime)
         f_handle = field.device(runtime, _lib.MODEL_SH)
-        tracker = runtime.tracker()
         a = to_struct(algorithm)
         dev_seeds = runtime.to_device(seeds)
         host_seeds = runtime.pinned(seeds.shape, np.float32)
         host_seeds[...] = seeds
-        torch.cuda.synchronize()
-        lengths = np.empty(n_job, np.uint32)
-        offsets = np.empty(n_job, np.uint64)
-        total = ctypes.c_uint64()
-        steps = ctypes.c_uint64()
-        kms = ctypes.c_float()
-        waves = ctypes.c_uint32()
-        launches = ctypes.c_uint32()
 
-        def run(i, on_host):
+        class Slot:
+            """One job in flight: a stream, its tracker and its host buffers."""
+
+            def __init__(self, rt):
+                self.rt = rt
+                self.stream = rt.stream
+                self.sh = ctypes.c_void_p(rt.stream_handle)
+                self.tracker = rt.tracker()
+                self.lengths = np.empty(n_job, np.uint32)
+                self.offsets = np.empty(n_job, np.uint64)
+                self.out_host = None
+
+        slots = [Slot(runtime)] + [Slot(tg.CudaRuntime(local_rank, stream=torch.cuda.Stream(local_rank),
+                                                       pool_points=pool)) for _ in range(in_flight - 1)]
+        torch.cuda.synchronize()
+
+        def run(slot, i, on_host):
+            total, steps = ctypes.c_uint64(), ctypes.c_uint64()
+            kms, waves, launches = ctypes.c_float(), ctypes.c_uint32(), ctypes.c_uint32()
             ptr = host_seeds.ctypes.data_as(ctypes.c_void_p) if on_host else ctypes.c_void_p(dev_seeds.data_ptr())
             _lib.check(lib.tg_tracker_run(
-                tracker, ctypes.byref(a), d_handle, f_handle, ptr, 1 if on_host else 0, n_job, args.batch,
+                slot.tracker, ctypes.byref(a), d_handle, f_handle, ptr, 1 if on_host else 0, n_job, args.batch,
                 rng_seeds[i].ctypes.data_as(ctypes.c_void_p), SAVE_AT, n_steps,
-                lengths.ctypes.data_as(ctypes.c_void_p), offsets.ctypes.data_as(ctypes.c_void_p),
-                ctypes.byref(total), ctypes.byref(steps), sh))
-            _lib.check(lib.tg_tracker_stats(tracker, ctypes.byref(kms), ctypes.byref(waves), ctypes.byref(launches)))
+                slot.lengths.ctypes.data_as(ctypes.c_void_p), slot.offsets.ctypes.data_as(ctypes.c_void_p),
+                ctypes.byref(total), ctypes.byref(steps), slot.sh))
+            _lib.check(lib.tg_tracker_stats(slot.tracker, ctypes.byref(kms), ctypes.byref(waves),
+                                            ctypes.byref(launches)))
             return int(steps.value), int(total.value), float(kms.value), int(launches.value), int(waves.value)
 
-        warm_points = 0
+        def leg(on_host, width):
+            """Time jobs warmup .. warmup+steps-1 with `width` of them in flight.
+
+            Slot k runs jobs k, k+width, ... one after another from its own host
+            thread, so the next job's blocks take the SMs the previous job's tail
+            frees.  The start event is recorded before any job is queued and every
+            other stream waits for it; the end event waits for every stream."""
+            ev_start, ev_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ev_start.record(slots[0].stream)
+            for sl in slots[1:width]:
+                sl.stream.wait_event(ev_start)
+            results = [None] * args.steps
+            errors = []
+
+            def worker(k):
+                slot = slots[k]
+                try:
+                    with slot.rt.device_scope():
+                        for j in range(k, args.steps, width):
+                            i = args.warmup + j
+                            st, pts, km, nl, nw = run(slot, i, on_host)
+                            if on_host:
+                                if slot.out_host is None or pts > slot.out_host.shape[0]:
+                                    slot.out_host = slot.rt.pinned((int(pts * 1.1) + 1024, 3), np.float32)
+                                _lib.check(lib.tg_tracker_copy_points(
+                                    slot.tracker, slot.out_host.ctypes.data_as(ctypes.c_void_p), 0, pts, 1,
+                                    slot.sh))
+                            results[j] = (st, pts, km, nl, nw)
+                except Exception as exc:  # re-raised by the caller after every worker ends
+                    errors.append(exc)
+
+            threads = [threading.Thread(target=worker, args=(k,)) for k in range(width)]
+            for t in threads:
+                t.start()
+            for t in threads:
+                t.join()
+            if errors:
+                raise errors[0]
+            for sl in slots[1:width]:
+                ev = torch.cuda.Event()
+                ev.record(sl.stream)
+                slots[0].stream.wait_event(ev)
+            ev_end.record(slots[0].stream)
+            torch.cuda.synchronize()
+            return ev_start.elapsed_time(ev_end), results
+
         for i in range(args.warmup):
-            warm_points = max(warm_points, run(i, on_host=False)[1])
-        out_host = runtime.pinned((int(warm_points * 1.25) + 1024, 3), np.float32)
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            run(slots[i % in_flight], i, on_host=False)
 
         sampler = ClockSampler(local_rank)
         with sampler:
-            # device-resident leg
+            # one job at a time: the tracking kernel's launches alone (roofline)
             if dist is not None:
                 dist.barrier()
-            torch.cuda.synchronize()
-            ev0.record(stream)
-            dev_steps = dev_points = n_launch = n_waves = 0
-            kernel_ms = 0.0
-            for i in range(args.warmup, args.warmup + args.steps):
-                s, p, k, nl, nw = run(i, on_host=False)
-                dev_steps += s
-                dev_points += p
-                kernel_ms += k
-                n_launch += nl
-                n_waves += nw
-            ev1.record(stream)
-            torch.cuda.synchronize()
-            dev_ms = ev0.elapsed_time(ev1)
+            single_ms, single = leg(False, 1)
+            kernel_ms = sum(r[2] for r in single)
+            single_steps = sum(r[0] for r in single)
+            n_launch = sum(r[3] for r in single)
+            n_waves = sum(r[4] for r in single)
             if dist is not None:
                 dist.barrier()
-
-            # end-to-end leg through the C ABI with host buffers
-            torch.cuda.synchronize()
-            ev0.record(stream)
-            e2e_steps = 0
-            h2d = d2h = 0
-            for i in range(args.warmup, args.warmup + args.steps):
-                s, p, _, _, _ = run(i, on_host=True)
-                if p > out_host.shape[0]:
-                    out_host = runtime.pinned((p, 3), np.float32)
-                _lib.check(lib.tg_tracker_copy_points(tracker, out_host.ctypes.data_as(ctypes.c_void_p), 0, p, 1, sh))
-                e2e_steps += s
-                h2d += seeds.nbytes + rng_seeds[i].nbytes
-                d2h += p * 12 + n_job * (4 + 8)
-            ev1.record(stream)
-            torch.cuda.synchronize()
-            e2e_ms = ev0.elapsed_time(ev1)
+            # device-resident leg, jobs overlapped
+            dev_ms, dev = leg(False, in_flight)
+            dev_steps = sum(r[0] for r in dev)
+            dev_points = sum(r[1] for r in dev)
+            if dist is not None:
+                dist.barrier()
+            # end-to-end leg through the C ABI with host buffers, jobs overlapped
+            e2e_ms, e2e = leg(True, in_flight)
+            e2e_steps = sum(r[0] for r in e2e)
+            h2d = sum(seeds.nbytes + rng_seeds[args.warmup + j].nbytes for j in range(args.steps))
+            d2h = sum(r[1] * 12 + n_job * (4 + 8) for r in e2e)
             if dist is not None:
                 dist.barrier()
 
-        # outside the timed region: the last timed run against the oracle
+        # outside the timed region: the last job of the end-to-end leg against the oracle
         parity = None
+        last = slots[(args.steps - 1) % in_flight]
         if not args.no_cpu_baseline and world == 1:
-            parity = parity_sample(lib, tracker, sh, algorithm, field, domain, seeds, args.batch,
-                                   rng_seeds[args.warmup + args.steps - 1], lengths, offsets)
+            parity = parity_sample(lib, last.tracker, last.sh, algorithm, field, domain, seeds, args.batch,
+                                   rng_seeds[args.warmup + args.steps - 1], last.lengths, last.offsets)
 
     if dist is not None:
-        (dev_ms, e2e_ms, kernel_ms), (dev_steps, e2e_steps, dev_points, n_launch, n_waves) = combine_ranks(
-            dist, [dev_ms, e2e_ms, kernel_ms], [dev_steps, e2e_steps, dev_points, n_launch, n_waves], "cuda")
+        (dev_ms, e2e_ms, kernel_ms, single_ms), (dev_steps, e2e_steps, dev_points, n_launch, n_waves,
+                                                 single_steps) = combine_ranks(
+            dist, [dev_ms, e2e_ms, kernel_ms, single_ms],
+            [dev_steps, e2e_steps, dev_points, n_launch, n_waves, single_steps], "cuda")
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -343,7 +395,8 @@ def run_ours(args):
 
     peak, peak_kind = measured_peaks()
     value = dev_steps / (dev_ms / 1e3)
-    kernel_steps_per_s = dev_steps / max(1, world) / (kernel_ms / 1e3)
+    # the tracking kernel's own rate, from the leg that runs one job at a time
+    kernel_steps_per_s = single_steps / max(1, world) / (kernel_ms / 1e3)
     achieved = kernel_steps_per_s * BYTES_PER_STEP / 1e9
     tps = traffic_per_step()
     line = {
@@ -367,6 +420,7 @@ def run_ours(args):
             "cache": "inputs larger than L2: 660 MB FOD volume, 126 MB L2",
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "rng": "MWC64X reference stream per batch",
+            "jobs_in_flight": in_flight,
         },
         "streamlines_per_s": n_job * args.steps * world / (dev_ms / 1e3),
         "points_per_step": dev_points / args.steps / max(1, world),
@@ -383,10 +437,16 @@ def run_ours(args):
             "peak": peak,
             "unit": "GB/s",
             "frac": achieved / peak,
-            "traffic": (tps * dev_steps / max(1, n_waves)) if tps is not None else None,
+            "traffic": (tps * single_steps / max(1, n_waves)) if tps is not None else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "bytes_per_step": BYTES_PER_STEP,
             "kernel_ms_per_step": kernel_ms / args.steps / max(1, world),
+            "launches_from": "the one-job-at-a-time leg (single_job)",
+        },
+        "single_job": {
+            "value": single_steps / (single_ms / 1e3),
+            "ms_per_step": single_ms / args.steps,
+            "note": "the same jobs one at a time: each tg_tracker_run returns before the next starts",
         },
         "clocks": sampler.summary(),
     }
