@@ -89,6 +89,10 @@ def parse_args():
     p.add_argument("--in-flight", type=int, default=2,
                    help="config1: jobs in flight (each on its own stream and tracker); one job's copies and "
                         "host work overlap the other's tracking")
+    p.add_argument("--compact-lanes", type=int, default=0,
+                   help="config1: tail compaction (tg_tracker_set_tuning): warps left with at most this many "
+                        "live streamlines after the queue drains hand them to a follow-up round; 0 = off")
+    p.add_argument("--compact-rounds", type=int, default=4, help="config1: follow-up rounds of tail compaction")
     p.add_argument("--workload", choices=["config1", "config0", "mixed", "config2", "serve", "tod", "connectome"],
                    default="config1",
                    help="config1 (default headline), the 64-job mixed workload, the DTI + mesh workload, or "
@@ -282,6 +286,8 @@ def run_ours(args):
                 self.stream = rt.stream
                 self.sh = ctypes.c_void_p(rt.stream_handle)
                 self.tracker = rt.tracker()
+                if args.compact_lanes > 0:
+                    rt.set_tuning(0, args.compact_lanes, args.compact_rounds)
                 self.lengths = np.empty(n_job, np.uint32)
                 self.offsets = np.empty(n_job, np.uint64)
                 self.out_host = None
@@ -434,6 +440,7 @@ def run_ours(args):
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "rng": "MWC64X reference stream per batch",
             "jobs_in_flight": in_flight,
+            "compact_lanes": args.compact_lanes,
         },
         "streamlines_per_s": n_job * args.steps * world / (dev_ms / 1e3),
         "points_per_step": dev_points / args.steps / max(1, world),
