@@ -93,6 +93,9 @@ def parse_args():
                    help="config1: tail compaction (tg_tracker_set_tuning): warps left with at most this many "
                         "live streamlines after the queue drains hand them to a follow-up round; 0 = off")
     p.add_argument("--compact-rounds", type=int, default=4, help="config1: follow-up rounds of tail compaction")
+    p.add_argument("--slice", type=int, default=None,
+                   help="config1: time slicing (tg_tracker_set_slicing): a streamline yields its lane every this "
+                        "many steps while other work waits; 0 = off; default: the library's")
     p.add_argument("--workload", choices=["config1", "config0", "mixed", "config2", "serve", "tod", "connectome"],
                    default="config1",
                    help="config1 (default headline), the 64-job mixed workload, the DTI + mesh workload, or "
@@ -288,6 +291,8 @@ def run_ours(args):
                 self.tracker = rt.tracker()
                 if args.compact_lanes > 0:
                     rt.set_tuning(0, args.compact_lanes, args.compact_rounds)
+                if args.slice is not None:
+                    rt.set_slicing(args.slice)
                 self.lengths = np.empty(n_job, np.uint32)
                 self.offsets = np.empty(n_job, np.uint64)
                 self.out_host = None
@@ -441,6 +446,7 @@ def run_ours(args):
             "rng": "MWC64X reference stream per batch",
             "jobs_in_flight": in_flight,
             "compact_lanes": args.compact_lanes,
+            "slice_steps": runtime.slicing(),
         },
         "streamlines_per_s": n_job * args.steps * world / (dev_ms / 1e3),
         "points_per_step": dev_points / args.steps / max(1, world),

@@ -224,6 +224,24 @@ int tg_tracker_set_tuning(tg_tracker* tracker, uint32_t blocks_per_sm, uint32_t 
 int tg_tracker_get_tuning(const tg_tracker* tracker, uint32_t* blocks_per_sm, uint32_t* compact_lanes,
                           uint32_t* compact_rounds);
 
+/* Time slicing of tg_tracker_run's persistent launch.  slice_steps 0: every
+ * lane tracks a streamline to its end before taking the next seed.  A power
+ * of two: a streamline whose step count reaches a multiple of slice_steps
+ * while other work waits (seeds not yet started, or streamlines already
+ * saved) is saved to a device queue and its lane takes the next work, seeds
+ * first, then the saved streamlines in the order they were saved.  Every
+ * seed then starts early and the long streamlines share the lanes
+ * round-robin, so the launch no longer ends with a long streamline that
+ * started last running on an otherwise idle GPU.  Runs whose step bound
+ * (tg_step_bound) does not exceed slice_steps are not sliced.  Results do
+ * not depend on this setting (a saved streamline carries its position,
+ * orientation, RNG state and output cursor).  The queue takes about 104
+ * bytes per seed of a sliced run.  Default 32768.  Returns
+ * TG_ERR_INVALID_ARGUMENT for other values.  No reference counterpart:
+ * scheduling only. */
+int tg_tracker_set_slicing(tg_tracker* tracker, uint32_t slice_steps);
+int tg_tracker_get_slicing(const tg_tracker* tracker, uint32_t* slice_steps);
+
 /* Continuous-batching server.  No reference counterpart (the reference
  * tracks one tg.tractogram call at a time).  Fields, domains and surfaces
  * stay resident as ordinary handles; requests (tg_job with HOST seeds and

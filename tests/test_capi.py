@@ -54,6 +54,8 @@ def test_invalid_arguments_fail_without_a_device():
     assert b"null" in lib.tg_last_error()
     with pytest.raises(ValueError):
         _lib.check(status)
+    assert lib.tg_tracker_set_slicing(None, 16) == _lib.TG_ERR_INVALID_ARGUMENT
+    assert lib.tg_tracker_get_slicing(None, None) == _lib.TG_ERR_INVALID_ARGUMENT
 
 
 def test_missing_library_fails_loudly(tmp_path, monkeypatch):

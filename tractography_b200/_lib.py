@@ -50,6 +50,8 @@ EXPORTS = (
     "tg_tracker_stats",
     "tg_tracker_set_tuning",
     "tg_tracker_get_tuning",
+    "tg_tracker_set_slicing",
+    "tg_tracker_get_slicing",
     "tg_tracker_copy_points",
     "tg_server_create",
     "tg_server_destroy",
@@ -157,6 +159,8 @@ def load() -> ctypes.CDLL:
         "tg_tracker_stats": ([P, ctypes.POINTER(F), ctypes.POINTER(U32), ctypes.POINTER(U32)], ctypes.c_int),
         "tg_tracker_set_tuning": ([P, U32, U32, U32], ctypes.c_int),
         "tg_tracker_get_tuning": ([P, ctypes.POINTER(U32), ctypes.POINTER(U32), ctypes.POINTER(U32)], ctypes.c_int),
+        "tg_tracker_set_slicing": ([P, U32], ctypes.c_int),
+        "tg_tracker_get_slicing": ([P, ctypes.POINTER(U32)], ctypes.c_int),
         "tg_tracker_copy_points": ([P, P, U64, U64, ctypes.c_int, P], ctypes.c_int),
         "tg_server_create": ([U64, U64, U32, U32, ctypes.POINTER(P)], ctypes.c_int),
         "tg_server_destroy": ([P], ctypes.c_int),

@@ -78,6 +78,15 @@ struct tg_tracker {
     uint32_t blocks_per_sm = 0;        // 0: the occupancy maximum
     uint32_t compact_lanes = 0;        // 0: no compaction (measured faster by default)
     uint32_t compact_rounds = 4;
+    // time slicing of tg_tracker_run (tg_tracker_set_slicing): the ring of
+    // saved streamlines, its seq and released words and its control words
+    uint32_t slice_steps = kDefaultSliceSteps;
+    LaneCarry* ring_items = nullptr;
+    size_t cap_ring = 0;
+    uint32_t* ring_flags = nullptr;    // seq then released, cap_ring each
+    size_t cap_ring_flags = 0;
+    unsigned int* ring_ctl = nullptr;  // head, tail, fault, spare
+    size_t cap_ring_ctl = 0;
     LaneCarry* carry[kClassKinds + 1][2] = {};
     size_t carry_cap[kClassKinds + 1] = {};
     unsigned int* carry_count = nullptr;   // 2 per slot
@@ -580,6 +589,9 @@ int tg_tracker_destroy(tg_tracker* t)
     cudaFree(t->seeds);
     cudaFree(t->batch_seeds);
     cudaFree(t->points);
+    cudaFree(t->ring_items);
+    cudaFree(t->ring_flags);
+    cudaFree(t->ring_ctl);
     if (t->ev_start) cudaEventDestroy(t->ev_start);
     if (t->ev_stop) cudaEventDestroy(t->ev_stop);
     for (int k = 0; k < kClassKinds; ++k) {
@@ -609,6 +621,22 @@ int tg_tracker_set_tuning(tg_tracker* t, uint32_t blocks_per_sm, uint32_t compac
     t->blocks_per_sm = blocks_per_sm;
     t->compact_lanes = compact_lanes;
     t->compact_rounds = compact_rounds;
+    return TG_OK;
+}
+
+int tg_tracker_set_slicing(tg_tracker* t, uint32_t slice_steps)
+{
+    if (t == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "tracker is null");
+    if (slice_steps > (1u << 30) || (slice_steps & (slice_steps - 1u)) != 0u)
+        return fail(TG_ERR_INVALID_ARGUMENT, "slice_steps must be 0 or a power of two up to 2^30");
+    t->slice_steps = slice_steps;
+    return TG_OK;
+}
+
+int tg_tracker_get_slicing(const tg_tracker* t, uint32_t* slice_steps)
+{
+    if (t == nullptr) return fail(TG_ERR_INVALID_ARGUMENT, "tracker is null");
+    if (slice_steps) *slice_steps = t->slice_steps;
     return TG_OK;
 }
 
@@ -785,6 +813,23 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
         st = tracker_carry(t, kClassKinds, (size_t)grid * block);
         if (st != TG_OK) return st;
     }
+    // slicing only where a streamline can outlast a slice
+    if (t->slice_steps > 0 && tp.max_steps > t->slice_steps) {
+        // every streamline live in a launch is in a lane or once in the ring
+        const size_t cap = (size_t)n_seeds + (size_t)grid * block + 1;
+        if (cap > 0xFFFFFFFFull) return fail(TG_ERR_INVALID_ARGUMENT, "too many seeds for time slicing");
+        TG_TRY(ensure(&t->ring_items, &t->cap_ring, cap));
+        TG_TRY(ensure(&t->ring_flags, &t->cap_ring_flags, 2 * cap));
+        TG_TRY(ensure(&t->ring_ctl, &t->cap_ring_ctl, 4));
+        TG_TRY(cudaMemsetAsync(t->ring_ctl, 0, 4 * sizeof(unsigned int), s));
+        pp.ring.items = t->ring_items;
+        pp.ring.seq = t->ring_flags;
+        pp.ring.released = t->ring_flags + cap;
+        pp.ring.ctl = t->ring_ctl;
+        pp.ring.capacity = (uint32_t)cap;
+        pp.ring.lanes = (uint32_t)grid * (uint32_t)block;
+        pp.slice_mask = t->slice_steps - 1u;
+    }
     unsigned int* ccount = t->carry_count + 2 * kClassKinds;
 
     t->h_len.resize(n_seeds);
@@ -818,6 +863,11 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
             pp.carry_out_count = ccount + (r & 1);
             pp.compact_lanes = t->compact_lanes;
             if (r < rounds) TG_TRY(cudaMemsetAsync(ccount + (r & 1), 0, sizeof(unsigned int), s));
+            if (pp.ring.items != nullptr) {
+                // an empty ring for each launch; the fault word spans the run
+                TG_TRY(cudaMemsetAsync(pp.ring.seq, 0, 2 * (size_t)pp.ring.capacity * sizeof(uint32_t), s));
+                TG_TRY(cudaMemsetAsync(pp.ring.ctl, 0, 2 * sizeof(unsigned int), s));
+            }
             TG_TRY(launch_track_persistent(field->d, pp, grid, block, s));
             t->launches += 1;
         }
@@ -899,8 +949,15 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
         first_wave = false;
     }
     unsigned long long steps = 0;
+    unsigned int ring_fault = 0;
     TG_TRY(cudaMemcpyAsync(&steps, t->counters + 1, sizeof steps, cudaMemcpyDeviceToHost, s));
+    if (pp.ring.items != nullptr)
+        TG_TRY(cudaMemcpyAsync(&ring_fault, pp.ring.ctl + 2, sizeof ring_fault, cudaMemcpyDeviceToHost, s));
     TG_TRY(cudaStreamSynchronize(s));
+    if (ring_fault != 0u)
+        return fail(TG_ERR_CUDA, std::string("time slicing: a bounded wait on the queue of saved streamlines ran "
+                                             "out (") + ((ring_fault & 1u) ? "slot" : "") +
+                                     ((ring_fault & 2u) ? " claim" : "") + ")");
     t->total_points = total;
     if (total_points) *total_points = total;
     if (total_steps) *total_steps = steps;

@@ -18,6 +18,27 @@ namespace tg {
 
 struct LaneCarry;   // tg_step.cuh
 
+// Default time slice of tg_tracker_run (tg_tracker_set_slicing), in steps.
+constexpr uint32_t kDefaultSliceSteps = 32768;
+
+// A FIFO of saved streamlines shared by one launch's lanes.  Ticket t
+// (taken from ctl[1]) is written to slot t % capacity, published by
+// seq[slot] = t + 1; a lane claims the oldest ticket (ctl[0]) only while it
+// is below ctl[1], and marks the slot free again by released[slot] = t + 1.
+// ctl[2]: nonzero when a bounded wait ran out (1: a slot's wait, 2: a
+// claim's retries; the run then fails).  seq,
+// released and ctl are zero at the launch.  capacity exceeds the number of
+// streamlines that can be live at once, so a ticket's slot was claimed long
+// before the ticket capacity later reuses it.
+struct TrackRing {
+    LaneCarry* items;
+    uint32_t* seq;
+    uint32_t* released;
+    unsigned int* ctl;
+    uint32_t capacity;
+    uint32_t lanes;      // lanes of the launch: claims in flight at most
+};
+
 constexpr int kChunkPoints = 32;   // points per output chunk (chunk = 32 x 12 B)
 
 // Device-resident image field (field.py:52-122): float32 coefficients,
@@ -111,6 +132,15 @@ struct PersistentParams {
     LaneCarry* carry_out;
     unsigned int* carry_out_count;
     uint32_t compact_lanes;
+    // Time slicing (tg_tracker_set_slicing): with ring.items set, a
+    // streamline whose step count reaches a multiple of slice_mask + 1 while
+    // other work waits (seeds left in the queue, or streamlines in the ring)
+    // is saved at the ring's tail and its lane takes the next work; lanes
+    // take seeds first, then the ring in order.  Every seed thus starts
+    // early and the long streamlines share the lanes round-robin, instead of
+    // a long streamline started last setting the end of the launch.
+    TrackRing ring;
+    uint32_t slice_mask;
 };
 
 // Many jobs queued at once (tg_multi.cu).  Job j covers global seed indices

@@ -92,7 +92,115 @@ __device__ __forceinline__ bool emit_point(const PersistentParams& pp, int32_t& 
     return true;
 }
 
-template <int MODEL, int LMAX, int ALGO, int DOM>
+// ------------------------------------------------------------ time slicing
+
+constexpr uint32_t kRingWaitLimit = 1u << 22;   // polls of a slot (64 ns apart) before a wait gives up
+constexpr uint32_t kRingClaimLimit = 1u << 20;  // lost claim races before a claim gives up
+constexpr uint32_t kRingTicketLimit = 0xF0000000u;
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Polls *p until it equals want, 64 ns apart, at most kRingWaitLimit times;
+// false (and the ring's fault word set) when the limit is reached.
+__device__ __forceinline__ bool ring_wait(const TrackRing& R, const uint32_t* p, uint32_t want)
+{
+    for (uint32_t k = 0; k < kRingWaitLimit; ++k) {
+        if (ld_acquire(p) == want) return true;
+        __nanosleep(64);
+    }
+    atomicOr(R.ctl + 2, 1u);
+    return false;
+}
+
+// Other work waiting: seeds left in the launch's queue, or saved
+// streamlines in the ring (tickets reserved and not yet claimed).
+__device__ __forceinline__ bool work_waiting(const PersistentParams& pp, unsigned long long n_items)
+{
+    const unsigned long long next = *reinterpret_cast<volatile const unsigned long long*>(pp.item_counter);
+    if (next < n_items) return true;
+    const uint32_t head = ld_relaxed(pp.ring.ctl);
+    const uint32_t tail = ld_relaxed(pp.ring.ctl + 1);
+    return head < tail && tail < kRingTicketLimit;
+}
+
+// Saves the lane's streamline at the ring's tail.  The slot's previous
+// ticket was claimed capacity tickets ago; the wait is for its reader to
+// have finished.
+__device__ __forceinline__ void ring_push(const TrackRing& R, const Lane& s, uint32_t item, int32_t chunk,
+                                          uint32_t fill)
+{
+    const uint32_t t = atomicAdd(R.ctl + 1, 1u);
+    const uint32_t slot = t % R.capacity;
+    if (t >= R.capacity && !ring_wait(R, R.released + slot, t - R.capacity + 1u)) return;
+    LaneCarry c;
+    lane_save(&c, s, item, chunk, fill);
+    const uint4* src = reinterpret_cast<const uint4*>(&c);
+    uint4* dst = reinterpret_cast<uint4*>(R.items + slot);
+#pragma unroll
+    for (int k = 0; k < (int)(sizeof(LaneCarry) / 16); ++k) __stcg(dst + k, src[k]);
+    st_release(R.seq + slot, t + 1u);
+}
+
+// Claims the ring's oldest saved streamline into the lane; false when the
+// ring holds none.  A ticket is claimed only below the tail, so its writer
+// has reserved it and is at most a few stores from publishing it.  With at
+// least `lanes` tickets between head and tail a plain increment of the head
+// cannot pass the tail (each lane has at most one claim in flight); with
+// fewer, the claim is a compare-and-swap that fails when another lane got
+// the ticket first.  (Compare-and-swap alone serialises the claims of
+// thousands of lanes, one success per round trip.)
+__device__ __forceinline__ bool ring_take(const TrackRing& R, Lane& s, uint32_t& item, int32_t& chunk,
+                                          uint32_t& fill)
+{
+    uint32_t h = 0;
+    bool claimed = false;
+    for (uint32_t k = 0; k < kRingClaimLimit && !claimed; ++k) {
+        h = ld_relaxed(R.ctl);
+        const uint32_t tail = ld_relaxed(R.ctl + 1);
+        if (h >= tail) return false;
+        if (tail - h >= R.lanes) {
+            h = atomicAdd(R.ctl, 1u);
+            claimed = true;
+        } else {
+            claimed = atomicCAS(R.ctl, h, h + 1u) == h;
+        }
+    }
+    if (!claimed) {
+        atomicOr(R.ctl + 2, 2u);
+        return false;
+    }
+    const uint32_t slot = h % R.capacity;
+    if (!ring_wait(R, R.seq + slot, h + 1u)) return false;
+    LaneCarry c;
+    const uint4* src = reinterpret_cast<const uint4*>(R.items + slot);
+    uint4* dst = reinterpret_cast<uint4*>(&c);
+#pragma unroll
+    for (int k = 0; k < (int)(sizeof(LaneCarry) / 16); ++k) dst[k] = __ldcg(src + k);
+    st_release(R.released + slot, h + 1u);
+    lane_restore(s, c, item, chunk, fill);
+    return true;
+}
+
+// SLICE: compiled with time slicing (pp.ring set) or without, so that the
+// plain form keeps its registers.
+template <int MODEL, int LMAX, int ALGO, int DOM, bool SLICE>
 __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>())) track_persistent_kernel(
     const PersistentParams pp)
 {
@@ -114,8 +222,11 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
     // Pull the next seed (or carried streamline); false when the queue is drained.
     auto fetch = [&]() -> bool {
         while (true) {
+            if (SLICE &&
+                *reinterpret_cast<volatile const unsigned long long*>(pp.item_counter) >= n_items)
+                return ring_take(pp.ring, s, item, chunk, fill);
             const unsigned long long it = atomicAdd(pp.item_counter, 1ull);
-            if (it >= n_items) return false;
+            if (it >= n_items) return SLICE && ring_take(pp.ring, s, item, chunk, fill);
             if (pp.carry_in != nullptr) {
                 lane_restore(s, pp.carry_in[it], item, chunk, fill);
                 return true;
@@ -166,28 +277,38 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
             if (__any_sync(0xffffffffu, route == 1)) hit = warp_leaves_hit(p.mesh, route == 1, g, list);
             if (testing) surface = route == 0 ? 0 : (route == 1 ? (hit ? 1 : 0) : -1);
         }
-        if (!live) continue;
-        bool done = s.n >= p.n_steps || s.steps >= p.max_steps;
-        bool overflow = false;
-        if (!done) {
-            float qx, qy, qz;
-            const int r = track_step<MODEL, LMAX, ALGO, CPAD, DOM>(p, s, c, qx, qy, qz, surface);
-            if (r == 0) {
-                done = true;
-            } else if (r == 2) {
-                if (emit_point(pp, chunk, fill, qx, qy, qz)) {
-                    s.n++;
-                } else {
+        bool refill = false;
+        if (live) {
+            bool done = s.n >= p.n_steps || s.steps >= p.max_steps;
+            bool overflow = false;
+            if (!done) {
+                float qx, qy, qz;
+                const int r = track_step<MODEL, LMAX, ALGO, CPAD, DOM>(p, s, c, qx, qy, qz, surface);
+                if (r == 0) {
                     done = true;
-                    overflow = true;
+                } else if (r == 2) {
+                    if (emit_point(pp, chunk, fill, qx, qy, qz)) {
+                        s.n++;
+                    } else {
+                        done = true;
+                        overflow = true;
+                    }
                 }
             }
+            if (done) {
+                pp.lengths[item] = overflow ? (s.n | kOverflowBit) : s.n;
+                if (!overflow) steps_total += s.steps;
+                refill = true;
+            } else if (SLICE && (s.steps & pp.slice_mask) == 0u && work_waiting(pp, n_items)) {
+                ring_push(pp.ring, s, item, chunk, fill);
+                refill = true;
+            }
         }
-        if (done) {
-            pp.lengths[item] = overflow ? (s.n | kOverflowBit) : s.n;
-            if (!overflow) steps_total += s.steps;
-            live = fetch();
-        }
+        // Time slicing: the warp's saved streamlines are all published
+        // before any of its lanes waits for a claimed one, so a lane never
+        // waits on a lane of its own warp.
+        if (SLICE) __syncwarp();
+        if (refill) live = fetch();
     }
     if (pp.steps_done != nullptr && steps_total != 0) atomicAdd(pp.steps_done, steps_total);
 }
@@ -259,7 +380,10 @@ template <int M, int L, int A, int D>
 struct PersistentLaunch {
     static cudaError_t run(const PersistentParams& p, int grid, int block, cudaStream_t stream)
     {
-        track_persistent_kernel<M, L, A, D><<<grid, block, 0, stream>>>(p);
+        if (p.ring.items != nullptr)
+            track_persistent_kernel<M, L, A, D, true><<<grid, block, 0, stream>>>(p);
+        else
+            track_persistent_kernel<M, L, A, D, false><<<grid, block, 0, stream>>>(p);
         return cudaGetLastError();
     }
 };
@@ -268,7 +392,7 @@ template <int M, int L, int A, int D>
 struct PersistentOccupancy {
     static cudaError_t run(int* blocks)
     {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, track_persistent_kernel<M, L, A, D>,
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, track_persistent_kernel<M, L, A, D, true>,
                                                              persistent_block_size(), 0);
     }
 };

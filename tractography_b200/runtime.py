@@ -73,6 +73,17 @@ class CudaRuntime:
         """Launch shape and tail compaction of the tracker (results do not depend on them)."""
         _lib.check(self.lib.tg_tracker_set_tuning(self.tracker(), blocks_per_sm, compact_lanes, compact_rounds))
 
+    def set_slicing(self, slice_steps: int) -> None:
+        """Time slicing of the tracker's persistent launch: 0 (off) or a power
+        of two, the steps after which a streamline yields its lane while other
+        work waits (results do not depend on it)."""
+        _lib.check(self.lib.tg_tracker_set_slicing(self.tracker(), slice_steps))
+
+    def slicing(self) -> int:
+        v = ctypes.c_uint32()
+        _lib.check(self.lib.tg_tracker_get_slicing(self.tracker(), ctypes.byref(v)))
+        return v.value
+
     def tuning(self) -> dict:
         b, c, r = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
         _lib.check(self.lib.tg_tracker_get_tuning(self.tracker(), ctypes.byref(b), ctypes.byref(c), ctypes.byref(r)))
