@@ -236,7 +236,7 @@ int tg_tracker_get_tuning(const tg_tracker* tracker, uint32_t* blocks_per_sm, ui
  * (tg_step_bound) does not exceed slice_steps are not sliced.  Results do
  * not depend on this setting (a saved streamline carries its position,
  * orientation, RNG state and output cursor).  The queue takes about 104
- * bytes per seed of a sliced run.  Default 32768.  Returns
+ * bytes per seed of a sliced run.  Default 65536.  Returns
  * TG_ERR_INVALID_ARGUMENT for other values.  No reference counterpart:
  * scheduling only. */
 int tg_tracker_set_slicing(tg_tracker* tracker, uint32_t slice_steps);

@@ -129,7 +129,7 @@ def test_sliced_closed_surface_run_equals_the_oracle():
 
 def test_slice_steps_must_be_a_power_of_two():
     rt = tg.CudaRuntime()
-    assert rt.slicing() == 32768
+    assert rt.slicing() == 65536
     for bad in (3, 100, (1 << 30) + 1, 1 << 31):
         with pytest.raises(ValueError):
             rt.set_slicing(bad)

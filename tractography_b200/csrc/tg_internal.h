@@ -19,7 +19,7 @@ namespace tg {
 struct LaneCarry;   // tg_step.cuh
 
 // Default time slice of tg_tracker_run (tg_tracker_set_slicing), in steps.
-constexpr uint32_t kDefaultSliceSteps = 32768;
+constexpr uint32_t kDefaultSliceSteps = 65536;
 
 // A FIFO of saved streamlines shared by one launch's lanes.  Ticket t
 // (taken from ctl[1]) is written to slot t % capacity, published by
