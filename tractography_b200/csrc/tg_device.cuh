@@ -316,7 +316,7 @@ __device__ __forceinline__ void update_orientation(const AlgoParams& a, const fl
         tz = fmaf(a.scale_noise, nz, a.scale_drift * dz);
     }
     exps2(ox, oy, oz, tx, ty, tz);
-    rng.step += 1u;
+    if constexpr (ALGO != kTransport) rng.step += 1u;
 }
 
 // ----------------------------------------------------- domain / field

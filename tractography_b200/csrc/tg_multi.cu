@@ -97,7 +97,7 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
             const unsigned long long k = atomicAdd(cls.counter, 1ull);
             if (k >= n_items) return false;
             if (mp.carry_in != nullptr) {
-                lane_restore(s, mp.carry_in[k], g, chunk, fill);
+                lane_restore<ALGO != kTransport>(s, mp.carry_in[k], g, chunk, fill);
                 J = mp.jobs + (upper_bound_u32(mp.job_base, mp.n_jobs + 1, g) - 1);
                 P = &J->t;
                 return true;
@@ -139,7 +139,8 @@ __device__ __forceinline__ unsigned long long drain_class(const MultiParams& mp,
         const unsigned active = __ballot_sync(0xffffffffu, live);
         if (active == 0u) break;
         if (mp.carry_out != nullptr && warp_should_compact(active, mp.compact_lanes)) {
-            if (live) lane_save(mp.carry_out + atomicAdd(mp.carry_out_count, 1u), s, g, chunk, fill);
+            if (live)
+                lane_save<ALGO != kTransport>(mp.carry_out + atomicAdd(mp.carry_out_count, 1u), s, g, chunk, fill);
             break;
         }
         if (!live) continue;

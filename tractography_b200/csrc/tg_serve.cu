@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
         const unsigned long long k = atomicAdd(sp.counter, 1ull);
         if (k < sp.n_carry) {
             const LaneCarry& cc = sp.carry_in[k];
-            lane_restore(s, cc, item, chunk, fill);
+            lane_restore<ALGO != kTransport>(s, cc, item, chunk, fill);
             slot = cc.job;
             J = sp.jobs + slot;
         } else {
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
         }
         if (chunk < 0 && !start()) {
             // no room in the pool now: hand the unstarted seed to the next epoch
-            lane_save(sp.carry_out + atomicAdd(sp.carry_out_count, 1u), s, item, -1, 0u, slot);
+            lane_save<ALGO != kTransport>(sp.carry_out + atomicAdd(sp.carry_out_count, 1u), s, item, -1, 0u, slot);
             return false;
         }
         return true;
@@ -255,7 +255,9 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
             if (__shfl_sync(0xffffffffu, now, 0) > deadline) budget = 0u;
         }
         if (budget == 0u) {
-            if (live) lane_save(sp.carry_out + atomicAdd(sp.carry_out_count, 1u), s, item, chunk, fill, slot);
+            if (live)
+                lane_save<ALGO != kTransport>(sp.carry_out + atomicAdd(sp.carry_out_count, 1u), s, item, chunk, fill,
+                                              slot);
             break;
         }
         budget -= 1u;

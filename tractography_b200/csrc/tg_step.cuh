@@ -280,6 +280,9 @@ struct __align__(16) LaneCarry {
     uint32_t job;            // job slot (multi-request serving); 0 otherwise
 };
 
+// RNG: the streamline draws random numbers (Diffusion); Transport draws
+// none, so its RNG state is neither carried nor kept in registers.
+template <bool RNG = true>
 __device__ __forceinline__ void lane_save(LaneCarry* dst, const Lane& s, uint32_t item, int32_t chunk,
                                           uint32_t fill, uint32_t job = 0u)
 {
@@ -288,21 +291,31 @@ __device__ __forceinline__ void lane_save(LaneCarry* dst, const Lane& s, uint32_
     c.px = s.px; c.py = s.py; c.pz = s.pz; c.time = s.time;
     c.ox = s.ox; c.oy = s.oy; c.oz = s.oz; c.lx = s.lx;
     c.ly = s.ly; c.lz = s.lz; c.n = s.n; c.steps = s.steps;
-    c.mwc_x = s.rng.mwc.x; c.mwc_c = s.rng.mwc.c; c.rng_step = s.rng.step; c.item = item;
-    c.rng_index = s.rng.index;
+    c.item = item;
+    if (RNG) {
+        c.mwc_x = s.rng.mwc.x; c.mwc_c = s.rng.mwc.c; c.rng_step = s.rng.step;
+        c.rng_index = s.rng.index;
+    } else {
+        c.mwc_x = 0u; c.mwc_c = 0u; c.rng_step = 0u;
+        c.rng_index = 0ull;
+    }
     c.chunk = chunk;
     c.fill = fill;
     *dst = c;
 }
 
+template <bool RNG = true>
 __device__ __forceinline__ void lane_restore(Lane& s, const LaneCarry& c, uint32_t& item, int32_t& chunk,
                                              uint32_t& fill)
 {
     s.px = c.px; s.py = c.py; s.pz = c.pz; s.time = c.time;
     s.ox = c.ox; s.oy = c.oy; s.oz = c.oz; s.lx = c.lx;
     s.ly = c.ly; s.lz = c.lz; s.n = c.n; s.steps = c.steps;
-    s.rng.mwc.x = c.mwc_x; s.rng.mwc.c = c.mwc_c; s.rng.step = c.rng_step; item = c.item;
-    s.rng.index = c.rng_index;
+    item = c.item;
+    if (RNG) {
+        s.rng.mwc.x = c.mwc_x; s.rng.mwc.c = c.mwc_c; s.rng.step = c.rng_step;
+        s.rng.index = c.rng_index;
+    }
     s.dvx = s.dvy = s.dvz = __int_as_float(0x7fc00000);
     s.fvx = s.fvy = s.fvz = __int_as_float(0x7fc00000);
     s.seed_state = 0u;

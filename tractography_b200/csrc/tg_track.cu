@@ -143,6 +143,7 @@ __device__ __forceinline__ bool work_waiting(const PersistentParams& pp, unsigne
 // Saves the lane's streamline at the ring's tail.  The slot's previous
 // ticket was claimed capacity tickets ago; the wait is for its reader to
 // have finished.
+template <bool RNG>
 __device__ __forceinline__ void ring_push(const TrackRing& R, const Lane& s, uint32_t item, int32_t chunk,
                                           uint32_t fill)
 {
@@ -150,7 +151,7 @@ __device__ __forceinline__ void ring_push(const TrackRing& R, const Lane& s, uin
     const uint32_t slot = t % R.capacity;
     if (t >= R.capacity && !ring_wait(R, R.released + slot, t - R.capacity + 1u)) return;
     LaneCarry c;
-    lane_save(&c, s, item, chunk, fill);
+    lane_save<RNG>(&c, s, item, chunk, fill);
     const uint4* src = reinterpret_cast<const uint4*>(&c);
     uint4* dst = reinterpret_cast<uint4*>(R.items + slot);
 #pragma unroll
@@ -166,6 +167,7 @@ __device__ __forceinline__ void ring_push(const TrackRing& R, const Lane& s, uin
 // fewer, the claim is a compare-and-swap that fails when another lane got
 // the ticket first.  (Compare-and-swap alone serialises the claims of
 // thousands of lanes, one success per round trip.)
+template <bool RNG>
 __device__ __forceinline__ bool ring_take(const TrackRing& R, Lane& s, uint32_t& item, int32_t& chunk,
                                           uint32_t& fill)
 {
@@ -194,7 +196,7 @@ __device__ __forceinline__ bool ring_take(const TrackRing& R, Lane& s, uint32_t&
 #pragma unroll
     for (int k = 0; k < (int)(sizeof(LaneCarry) / 16); ++k) dst[k] = __ldcg(src + k);
     st_release(R.released + slot, h + 1u);
-    lane_restore(s, c, item, chunk, fill);
+    lane_restore<RNG>(s, c, item, chunk, fill);
     return true;
 }
 
@@ -224,11 +226,11 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
         while (true) {
             if (SLICE &&
                 *reinterpret_cast<volatile const unsigned long long*>(pp.item_counter) >= n_items)
-                return ring_take(pp.ring, s, item, chunk, fill);
+                return ring_take<ALGO != kTransport>(pp.ring, s, item, chunk, fill);
             const unsigned long long it = atomicAdd(pp.item_counter, 1ull);
-            if (it >= n_items) return SLICE && ring_take(pp.ring, s, item, chunk, fill);
+            if (it >= n_items) return SLICE && ring_take<ALGO != kTransport>(pp.ring, s, item, chunk, fill);
             if (pp.carry_in != nullptr) {
-                lane_restore(s, pp.carry_in[it], item, chunk, fill);
+                lane_restore<ALGO != kTransport>(s, pp.carry_in[it], item, chunk, fill);
                 return true;
             }
             item = pp.item_ids != nullptr ? pp.item_ids[it] : (uint32_t)it;
@@ -255,7 +257,9 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
         const unsigned active = __ballot_sync(0xffffffffu, live);
         if (active == 0u) break;
         if (pp.carry_out != nullptr && warp_should_compact(active, pp.compact_lanes)) {
-            if (live) lane_save(pp.carry_out + atomicAdd(pp.carry_out_count, 1u), s, item, chunk, fill);
+            if (live)
+                lane_save<ALGO != kTransport>(pp.carry_out + atomicAdd(pp.carry_out_count, 1u), s, item, chunk,
+                                              fill);
             break;
         }
         // Closed surface: the segment tests of this iteration, done here while
@@ -300,7 +304,7 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
                 if (!overflow) steps_total += s.steps;
                 refill = true;
             } else if (SLICE && (s.steps & pp.slice_mask) == 0u && work_waiting(pp, n_items)) {
-                ring_push(pp.ring, s, item, chunk, fill);
+                ring_push<ALGO != kTransport>(pp.ring, s, item, chunk, fill);
                 refill = true;
             }
         }
