@@ -84,7 +84,7 @@ static float randn(uint32_t s[2])                    /* core.cl:240-245 */
 }
 
 /* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter-based stream
- * used by the optional keyed mode (north-star item (b)). */
+ * keyed by (seed index, step), used by the optional keyed mode. */
 void tgo_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
 {
     uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
