@@ -226,7 +226,9 @@ int tg_tracker_get_tuning(const tg_tracker* tracker, uint32_t* blocks_per_sm, ui
 
 /* Time slicing of tg_tracker_run's persistent launch.  slice_steps 0: every
  * lane tracks a streamline to its end before taking the next seed.  A power
- * of two: a streamline whose step count reaches a multiple of slice_steps
+ * of two: the slice is K saved points, K the largest power of two whose
+ * points take at most slice_steps steps (by the most steps that can separate
+ * two saved points); a streamline whose point count reaches a multiple of K
  * while other work waits (seeds not yet started, or streamlines already
  * saved) is saved to a device queue and its lane takes the next work, seeds
  * first, then the saved streamlines in the order they were saved.  Every

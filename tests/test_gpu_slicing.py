@@ -1,11 +1,13 @@
 """Time slicing of the persistent tracker (tg_tracker_set_slicing).
 
-A streamline that reaches a multiple of slice_steps while other work waits
-is saved to a device queue and resumed later by whichever lane takes it.
-Slices far shorter than the streamlines force thousands of saves and
-resumes per run (with 2-step slices, hundreds of thousands, so that the
-queue's slots are reused several times); every result must still equal the
-oracle's, bit for bit, and the run without slicing.  Covered: the SH image path (Diffusion and
+A streamline whose saved points reach a multiple of the slice (slice_steps
+in points: the largest power of two whose points take at most slice_steps
+steps) while other work waits is saved to a device queue and resumed later
+by whichever lane takes it.  Slices far shorter than the streamlines force
+thousands of saves and resumes per run (with 2-step slices, one point per
+slice: hundreds of thousands, so that the queue's slots are reused several
+times); every result must still equal the oracle's, bit for bit, and the
+run without slicing.  Covered: the SH image path (Diffusion and
 Transport), the tensor closed-surface path, slicing together with tail
 compaction, and slicing across retry waves of a point pool that is too
 small.
@@ -55,10 +57,10 @@ def _stats(runtime):
     return waves.value
 
 
-@pytest.mark.parametrize("kind,slice_steps", [("diffusion", 16), ("diffusion", 256), ("transport", 64),
-                                              ("diffusion", 2)])
-def test_sliced_runs_equal_the_oracle_and_the_unsliced_run(kind, slice_steps):
-    field, domain, seeds = small_config0(n_voxels=16, n_seeds=2100, seed=8)
+@pytest.mark.parametrize("kind,slice_steps,n_seeds", [("diffusion", 16, 2100), ("diffusion", 256, 2100),
+                                                      ("transport", 64, 2100), ("diffusion", 2, 6300)])
+def test_sliced_runs_equal_the_oracle_and_the_unsliced_run(kind, slice_steps, n_seeds):
+    field, domain, seeds = small_config0(n_voxels=16, n_seeds=n_seeds, seed=8)
     n_steps = 120
     plain_rt = tg.CudaRuntime()
     plain_rt.set_slicing(0)
@@ -71,9 +73,9 @@ def test_sliced_runs_equal_the_oracle_and_the_unsliced_run(kind, slice_steps):
     assert np.array_equal(sliced.offsets, plain.offsets)
     assert bits_equal(sliced.points, plain.points)
     assert sliced.steps == plain.steps
-    # streamlines run several slices each (~300 steps on average); with
-    # 2-step slices the queue's slots are reused several times over (its
-    # capacity is the seeds plus the launch's lanes)
+    # streamlines run several slices each (~300 steps, ~60 points on
+    # average); with one-point slices the queue's ~380k saves reuse its slots
+    # several times over (its capacity is the seeds plus the launch's lanes)
     assert plain.steps / len(seeds) > 4 * min(slice_steps, 64)
     _check_oracle(sliced, rng, _sh_job(kind), domain, field, seeds, n_steps)
 

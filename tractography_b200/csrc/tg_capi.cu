@@ -828,7 +828,13 @@ int tg_tracker_run(tg_tracker* t, const tg_algorithm* algorithm, const tg_domain
         pp.ring.ctl = t->ring_ctl;
         pp.ring.capacity = (uint32_t)cap;
         pp.ring.lanes = (uint32_t)grid * (uint32_t)block;
-        pp.slice_mask = t->slice_steps - 1u;
+        // the slice in saved points: the largest power of two whose points
+        // take at most slice_steps steps (steps_per_point_bound each)
+        const uint64_t per_point = std::max<uint64_t>(1, steps_per_point_bound(algorithm->step_size, save_at));
+        const uint64_t points = std::max<uint64_t>(1, t->slice_steps / per_point);
+        uint32_t slice_points = 1;
+        while ((uint64_t)slice_points * 2 <= points && slice_points < (1u << 30)) slice_points *= 2;
+        pp.slice_mask = slice_points - 1u;
     }
     unsigned int* ccount = t->carry_count + 2 * kClassKinds;
 

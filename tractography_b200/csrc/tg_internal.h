@@ -133,10 +133,10 @@ struct PersistentParams {
     unsigned int* carry_out_count;
     uint32_t compact_lanes;
     // Time slicing (tg_tracker_set_slicing): with ring.items set, a
-    // streamline whose step count reaches a multiple of slice_mask + 1 while
-    // other work waits (seeds left in the queue, or streamlines in the ring)
-    // is saved at the ring's tail and its lane takes the next work; lanes
-    // take seeds first, then the ring in order.  Every seed thus starts
+    // streamline whose point count reaches a multiple of slice_mask + 1
+    // while other work waits (seeds left in the queue, or streamlines in the
+    // ring) is saved at the ring's tail and its lane takes the next work;
+    // lanes take seeds first, then the ring in order.  Every seed thus starts
     // early and the long streamlines share the lanes round-robin, instead of
     // a long streamline started last setting the end of the launch.
     TrackRing ring;

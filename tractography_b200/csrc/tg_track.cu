@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
             if (testing) surface = route == 0 ? 0 : (route == 1 ? (hit ? 1 : 0) : -1);
         }
         bool refill = false;
+        bool slice_end = false;
         if (live) {
             bool done = s.n >= p.n_steps || s.steps >= p.max_steps;
             bool overflow = false;
@@ -293,6 +294,8 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
                 } else if (r == 2) {
                     if (emit_point(pp, chunk, fill, qx, qy, qz)) {
                         s.n++;
+                        // a slice ends on a saved point: no test on the other steps
+                        if (SLICE && (s.n & pp.slice_mask) == 0u) slice_end = true;
                     } else {
                         done = true;
                         overflow = true;
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(128, (persistent_min_blocks<MODEL, LMAX, DOM>(
                 pp.lengths[item] = overflow ? (s.n | kOverflowBit) : s.n;
                 if (!overflow) steps_total += s.steps;
                 refill = true;
-            } else if (SLICE && (s.steps & pp.slice_mask) == 0u && work_waiting(pp, n_items)) {
+            } else if (SLICE && slice_end && work_waiting(pp, n_items)) {
                 ring_push<ALGO != kTransport>(pp.ring, s, item, chunk, fill);
                 refill = true;
             }
