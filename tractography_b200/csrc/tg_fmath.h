@@ -201,11 +201,14 @@ TGM_FN float tgm_logf(float x_in)
 /*
  * log for positive, finite, normal x -- the tracking step's arguments:
  * Box-Muller's uniform in [2^-24, 1) and 1 + e^{kx} in [1, 1 + e^30].
- * Same series as tgm_logf, without its special-value and subnormal
- * handling; the reduction x = m 2^e, m in [sqrt(1/2), sqrt(2)), comes from
- * one integer subtraction: with B the bits of sqrt(1/2), d = bits(x) - B,
- * m has the bits B + (d mod 2^23) (a carry out of the mantissa field lifts
- * m into [1, sqrt(2))) and e = floor(d / 2^23).
+ * The reduction x = m 2^e, m in [sqrt(1/2), sqrt(2)), comes from one
+ * integer subtraction: with B the bits of sqrt(1/2), d = bits(x) - B, m has
+ * the bits B + (d mod 2^23) (a carry out of the mantissa field lifts m into
+ * [1, sqrt(2))) and e = floor(d / 2^23).  Then log m = log(1 + f), f = m - 1
+ * exact, as f - f^2/2 + f^3 Q(f) with Q of degree 7 fitted to the relative
+ * error on [sqrt(1/2) - 1, sqrt(2) - 1] (gen_log_coefficients.py): no
+ * division, unlike tgm_logf's series in f / (2 + f).  Within one ulp of the
+ * correctly rounded logarithm on the floats tests/test_math.py checks.
  */
 TGM_FN float tgm_log_pos(float x)
 {
@@ -213,14 +216,16 @@ TGM_FN float tgm_log_pos(float x)
     const int e = (int)((d + 0x3f800000u) >> 23) - 127;
     const float m = tgm_u2f((d & 0x007fffffu) + 0x3f3504f3u);
     const float f = m - 1.0f;
-    const float s = f / (2.0f + f);
-    const float z = s * s;
-    float p = 0x1.c71c72p-4f;                         /* 1/9 */
-    p = fmaf(p, z, 0x1.24924ap-3f);                   /* 1/7 */
-    p = fmaf(p, z, 0x1.99999ap-3f);                   /* 1/5 */
-    p = fmaf(p, z, 0x1.555556p-2f);                   /* 1/3 */
-    const float two_s = s + s;
-    const float logm = fmaf(two_s * z, p, two_s);
+    float q = -0x1.38b4ccp-4f;                        /* Q7 */
+    q = fmaf(q, f, 0x1.055b46p-3f);                   /* Q6 */
+    q = fmaf(q, f, -0x1.0d8552p-3f);                  /* Q5 */
+    q = fmaf(q, f, 0x1.22da22p-3f);                   /* Q4 */
+    q = fmaf(q, f, -0x1.547244p-3f);                  /* Q3 */
+    q = fmaf(q, f, 0x1.99a008p-3f);                   /* Q2 */
+    q = fmaf(q, f, -0x1.000228p-2f);                  /* Q1 */
+    q = fmaf(q, f, 0x1.555554p-2f);                   /* Q0 */
+    const float t = fmaf(f, q, -0.5f);
+    const float logm = fmaf(f * f, t, f);
     const float ef = (float)e;
     return fmaf(ef, TGM_LN2_HI, fmaf(ef, TGM_LN2_LO, logm));
 }
