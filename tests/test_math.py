@@ -154,3 +154,22 @@ def test_philox_known_answer(oracle):
     assert list(oracle.philox([0, 0, 0, 0], [0, 0])) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
     assert list(oracle.philox([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2)) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6,
                                                                       0x6D5451FD]
+
+
+def test_log_coefficients_match_their_generator():
+    """tgm_log_pos's polynomial is the one gen_log_coefficients.py fits."""
+    import importlib.util
+    import re
+    from pathlib import Path
+
+    csrc = Path(__file__).resolve().parents[1] / "tractography_b200" / "csrc"
+    spec = importlib.util.spec_from_file_location("gen_log_coefficients", csrc / "gen_log_coefficients.py")
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    q, _ = gen.fit()
+    text = (csrc / "tg_fmath.h").read_text()
+    body = text[text.index("TGM_FN float tgm_log_pos"):text.index("TGM_FN float tgm_exp_upto30")]
+    found = {int(k): float.fromhex(v) for v, k in re.findall(r"(-?0x[0-9a-f.]+p-?\d+)f\);?\s*/\* Q(\d) \*/", body)}
+    found.update({int(k): float.fromhex(v) for v, k in re.findall(r"q = (-?0x[0-9a-f.]+p-?\d+)f;\s*/\* Q(\d) \*/", body)})
+    assert sorted(found) == list(range(8))
+    assert all(np.float32(found[k]) == q[k] for k in range(8))
