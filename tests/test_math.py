@@ -156,20 +156,21 @@ def test_philox_known_answer(oracle):
                                                                       0x6D5451FD]
 
 
-def test_log_coefficients_match_their_generator():
-    """tgm_log_pos's polynomial is the one gen_log_coefficients.py fits."""
+def test_polynomial_coefficients_match_their_generator():
+    """The fitted polynomials of tg_fmath.h are the ones gen_fmath_coefficients.py fits."""
     import importlib.util
     import re
     from pathlib import Path
 
     csrc = Path(__file__).resolve().parents[1] / "tractography_b200" / "csrc"
-    spec = importlib.util.spec_from_file_location("gen_log_coefficients", csrc / "gen_log_coefficients.py")
+    spec = importlib.util.spec_from_file_location("gen_fmath_coefficients", csrc / "gen_fmath_coefficients.py")
     gen = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(gen)
-    q, _ = gen.fit()
     text = (csrc / "tg_fmath.h").read_text()
-    body = text[text.index("TGM_FN float tgm_log_pos"):text.index("TGM_FN float tgm_exp_upto30")]
-    found = {int(k): float.fromhex(v) for v, k in re.findall(r"(-?0x[0-9a-f.]+p-?\d+)f\);?\s*/\* Q(\d) \*/", body)}
-    found.update({int(k): float.fromhex(v) for v, k in re.findall(r"q = (-?0x[0-9a-f.]+p-?\d+)f;\s*/\* Q(\d) \*/", body)})
-    assert sorted(found) == list(range(8))
-    assert all(np.float32(found[k]) == q[k] for k in range(8))
+    tagged = {}
+    for value, tag, k in re.findall(r"(-?0x[0-9a-f.]+p-?\d+|-0\.5)f[);]*\s*/\* ([QSCPK])(\d) \*/", text):
+        tagged.setdefault(tag, {})[int(k)] = float.fromhex(value) if value.startswith(("0x", "-0x")) else float(value)
+    for tag, name in (("Q", "log"), ("S", "sin"), ("C", "cos"), ("P", "expc"), ("K", "expk")):
+        q, _ = gen.fit(name)
+        assert sorted(tagged[tag]) == list(range(len(q))), tag
+        assert all(np.float32(tagged[tag][k]) == q[k] for k in range(len(q))), tag

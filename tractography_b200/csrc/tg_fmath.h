@@ -206,7 +206,7 @@ TGM_FN float tgm_logf(float x_in)
  * the bits B + (d mod 2^23) (a carry out of the mantissa field lifts m into
  * [1, sqrt(2))) and e = floor(d / 2^23).  Then log m = log(1 + f), f = m - 1
  * exact, as f - f^2/2 + f^3 Q(f) with Q of degree 7 fitted to the relative
- * error on [sqrt(1/2) - 1, sqrt(2) - 1] (gen_log_coefficients.py): no
+ * error on [sqrt(1/2) - 1, sqrt(2) - 1] (gen_fmath_coefficients.py): no
  * division, unlike tgm_logf's series in f / (2 + f).  Within one ulp of the
  * correctly rounded logarithm on the floats tests/test_math.py checks.
  */
@@ -256,26 +256,23 @@ TGM_FN float tgm_exp_upto30(float x_in)
 /*
  * The exponential map's factors (core.cl:101-109) from n2 = |t|^2 > 0:
  * c = cos(n) and k = sin(n) / n with n = sqrt(n2).  For n2 < 1 both are
- * Taylor series in n2 (cos to n^12, sin(n)/n to n^12 / 13!; truncation
- * below 1.2e-11), which needs neither the square root, the range reduction
- * nor the division; larger angles take the general path.
+ * 1 + n2 times a cubic in n2 fitted to the relative error on [0, 1)
+ * (gen_fmath_coefficients.py; fits within 2^-30), which needs neither the
+ * square root, the range reduction nor the division; larger angles take
+ * the general path.
  */
 TGM_FN void tgm_exps2_factors(float n2, float* c_out, float* k_out)
 {
     if (n2 < 1.0f) {
-        float pc = 0x1.1eed8ep-29f;                 /*  1/12! */
-        pc = fmaf(pc, n2, -0x1.27e4fcp-22f);        /* -1/10! */
-        pc = fmaf(pc, n2, 0x1.a01a02p-16f);         /*  1/8!  */
-        pc = fmaf(pc, n2, -0x1.6c16c2p-10f);        /* -1/6!  */
-        pc = fmaf(pc, n2, 0x1.555556p-5f);          /*  1/4!  */
-        pc = fmaf(pc, n2, -0.5f);                   /* -1/2!  */
+        float pc = 0x1.94a4c6p-16f;                 /* P3 */
+        pc = fmaf(pc, n2, -0x1.6beef6p-10f);        /* P2 */
+        pc = fmaf(pc, n2, 0x1.5554e6p-5f);          /* P1 */
+        pc = fmaf(pc, n2, -0x1.fffffep-2f);         /* P0 */
         *c_out = fmaf(pc, n2, 1.0f);
-        float pk = 0x1.612462p-33f;                 /*  1/13! */
-        pk = fmaf(pk, n2, -0x1.ae6456p-26f);        /* -1/11! */
-        pk = fmaf(pk, n2, 0x1.71de3ap-19f);         /*  1/9!  */
-        pk = fmaf(pk, n2, -0x1.a01a02p-13f);        /* -1/7!  */
-        pk = fmaf(pk, n2, 0x1.111112p-7f);          /*  1/5!  */
-        pk = fmaf(pk, n2, -0x1.555556p-3f);         /* -1/3!  */
+        float pk = 0x1.69b0f6p-19f;                 /* K3 */
+        pk = fmaf(pk, n2, -0x1.9ffe56p-13f);        /* K2 */
+        pk = fmaf(pk, n2, 0x1.1110ecp-7f);          /* K1 */
+        pk = fmaf(pk, n2, -0x1.555556p-3f);         /* K0 */
         *k_out = fmaf(pk, n2, 1.0f);
     } else {
         const float n = sqrtf(n2);
@@ -321,8 +318,9 @@ TGM_FN void tgm_softplus(float x, float k, float inv_k, float* value, float* der
  * that Box-Muller turns into an angle, core.cl:240-245).  The quarter turns
  * q = round(k / 2^22) come out exactly in integer arithmetic; the remainder
  * |r| <= 2^21 becomes an angle |t| <= pi/4 by one multiplication, and
- * cos(t + q pi/2) is cos t, -sin t, -cos t or sin t (series as in
- * tgm_sincosf).  No float argument reduction is needed.
+ * cos(t + q pi/2) is cos t, -sin t, -cos t or sin t, each a polynomial in
+ * t^2 fitted to the relative error on |t| <= pi/4
+ * (gen_fmath_coefficients.py).  No float argument reduction is needed.
  */
 #define TGM_TWO_PI_2M24 0x1.921fb6p-22f   /* float(2 pi) / 2^24, exact scaling */
 TGM_FN float tgm_cos2pi_u24(uint32_t k)
@@ -331,16 +329,14 @@ TGM_FN float tgm_cos2pi_u24(uint32_t k)
     const int32_t r = (int32_t)k - (int32_t)(q << 22);
     const float t = (float)r * TGM_TWO_PI_2M24;
     const float t2 = t * t;
-    float ps = 0x1.71de3ap-19f;                  /*  1/9! */
-    ps = fmaf(ps, t2, -0x1.a01a02p-13f);         /* -1/7! */
-    ps = fmaf(ps, t2, 0x1.111112p-7f);           /*  1/5! */
-    ps = fmaf(ps, t2, -0x1.555556p-3f);          /* -1/3! */
+    float ps = -0x1.9943e0p-13f;                 /* S2 */
+    ps = fmaf(ps, t2, 0x1.11073ap-7f);           /* S1 */
+    ps = fmaf(ps, t2, -0x1.555546p-3f);          /* S0 */
     const float st = fmaf(t * t2, ps, t);
-    float pc = -0x1.27e4fcp-22f;                 /* -1/10! */
-    pc = fmaf(pc, t2, 0x1.a01a02p-16f);          /*  1/8!  */
-    pc = fmaf(pc, t2, -0x1.6c16c2p-10f);         /* -1/6!  */
-    pc = fmaf(pc, t2, 0x1.555556p-5f);           /*  1/4!  */
-    pc = fmaf(pc, t2, -0.5f);
+    float pc = 0x1.9916a0p-16f;                  /* C3 */
+    pc = fmaf(pc, t2, -0x1.6c07f2p-10f);         /* C2 */
+    pc = fmaf(pc, t2, 0x1.55553cp-5f);           /* C1 */
+    pc = fmaf(pc, t2, -0.5f);                    /* C0 */
     const float ct = fmaf(t2, pc, 1.0f);
     const float c = (q & 1u) ? st : ct;
     return ((q + 1u) & 2u) ? -c : c;
