@@ -39,7 +39,7 @@ def test_exp_within_two_ulp(oracle):
 
 def test_log_of_positive_normal_arguments_within_one_ulp(oracle):
     """The step's logarithm (Box-Muller's uniform in [2^-24, 1), 1 + e^{kx} up to 1 + e^30):
-    the reduced argument's polynomial (gen_log_coefficients.py) stays within one ulp."""
+    the reduced argument's polynomial (gen_fmath_coefficients.py) stays within one ulp."""
     rng = np.random.default_rng(1)
     x = np.concatenate([
         np.arange(1, 1 << 24, 7, dtype=np.float64).astype(np.float32) * np.float32(2.0 ** -24),
