@@ -262,7 +262,8 @@ def math(which, x):
     x = np.ascontiguousarray(x, dtype=np.float32)
     out = np.zeros_like(x)
     code = {"sin": 0, "cos": 1, "exp": 2, "log": 3, "exps2_cos": 4, "exps2_sinc": 5, "softplus": 6,
-            "softplus_slope": 7, "softplus_inv_floor": 8, "cos2pi_u24": 9, "log_pos": 10, "exp_upto30": 11}[which]
+            "softplus_slope": 7, "softplus_inv_floor": 8, "cos2pi_u24": 9, "log_pos": 10, "exp_upto30": 11,
+            "rsqrt_pos": 12}[which]
     lib().tgo_math(code, _ptr(x), x.size, _ptr(out))
     return out
 

@@ -135,8 +135,15 @@ static frame_t frame_of(float x, float y, float z)
     const float r2 = fmaf(z, z, rho2);
     if (fabsf(r2 - 1.0f) < 0x1p-14f) {               /* near unit: 1/r = 1.5 - r^2/2 */
         const float ir = fmaf(-0.5f, r2, 1.5f);
-        const float rho = sqrtf(rho2);
         f.ct = fminf(fmaxf(z * ir, -1.0f), 1.0f);
+        if (rho2 >= 0x1p-100f) {                     /* 1/rho by tgm_rsqrt_pos */
+            const float irho = tgm_rsqrt_pos(rho2);
+            f.st = fminf((rho2 * irho) * ir, 1.0f);
+            f.cp = x * irho;
+            f.sp = y * irho;
+            return f;
+        }
+        const float rho = sqrtf(rho2);
         f.st = fminf(rho * ir, 1.0f);
         if (rho > 0.0f) {
             const float irho = 1.0f / rho;
@@ -1135,6 +1142,7 @@ void tgo_math(int which, const float* x, uint32_t n, float* out)
         case 9: out[i] = tgm_cos2pi_u24((uint32_t)x[i]); break;
         case 10: out[i] = tgm_log_pos(x[i]); break;
         case 11: out[i] = tgm_exp_upto30(x[i]); break;
+        case 12: out[i] = tgm_rsqrt_pos(x[i]); break;
         default: out[i] = x[i]; break;
         }
     }

@@ -174,3 +174,14 @@ def test_polynomial_coefficients_match_their_generator():
         q, _ = gen.fit(name)
         assert sorted(tagged[tag]) == list(range(len(q))), tag
         assert all(np.float32(tagged[tag][k]) == q[k] for k in range(len(q))), tag
+
+
+def test_reciprocal_square_root_within_two_ulp(oracle):
+    """The orientation frame's 1/rho: Lomont's estimate and three Newton steps."""
+    rng = np.random.default_rng(3)
+    x = np.concatenate([np.linspace(0.25, 4.0, 2_000_001, dtype=np.float32),
+                        (2.0 ** rng.uniform(-100, 60, 1_000_000)).astype(np.float32),
+                        np.array([2.0 ** -100, 1.0, 2.0, np.nextafter(np.float32(1.0), np.float32(0.0))],
+                                 np.float32)])
+    err = ulp_error(oracle.math("rsqrt_pos", x), 1.0 / np.sqrt(x.astype(np.float64)))
+    assert err.max() <= 2.0, (float(err.max()), x[np.argmax(err)])

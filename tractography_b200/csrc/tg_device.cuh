@@ -146,9 +146,11 @@ struct Frame {
 // ct = z/r, st = rho/r, cp = x/rho, sp = y/rho.  Orientations leave the
 // exponential map with |o|^2 = 1 within a few ulp; for |r^2 - 1| < 2^-14,
 // 1/r = 1.5 - r^2/2 to within 1.4e-9 relative (its expansion about 1), far
-// inside binary32 rounding.  Otherwise both reciprocals come from one
-// division, 1/r = rho q and 1/rho = r q with q = 1/(r rho); on the axis
-// (r rho rounds to 0) phi is taken as 0.
+// inside binary32 rounding, and 1/rho comes from tgm_rsqrt_pos (rho^2 at
+// least 2^-100; nearer the axis from a square root and a division).
+// Otherwise both reciprocals come from one division, 1/r = rho q and
+// 1/rho = r q with q = 1/(r rho); on the axis (r rho rounds to 0) phi is
+// taken as 0.
 __device__ __forceinline__ Frame frame_of(float x, float y, float z)
 {
     Frame f;
@@ -156,8 +158,16 @@ __device__ __forceinline__ Frame frame_of(float x, float y, float z)
     const float r2 = fmaf(z, z, rho2);
     if (fabsf(r2 - 1.0f) < 0x1p-14f) {
         const float ir = fmaf(-0.5f, r2, 1.5f);
-        const float rho = sqrtf(rho2);
         f.ct = fminf(fmaxf(z * ir, -1.0f), 1.0f);
+        if (rho2 >= 0x1p-100f) {
+            // 1/rho without a square root or a division; rho = rho2 / rho
+            const float irho = tgm_rsqrt_pos(rho2);
+            f.st = fminf((rho2 * irho) * ir, 1.0f);
+            f.cp = x * irho;
+            f.sp = y * irho;
+            return f;
+        }
+        const float rho = sqrtf(rho2);
         f.st = fminf(rho * ir, 1.0f);
         if (rho > 0.0f) {
             const float irho = 1.0f / rho;
